@@ -1,0 +1,271 @@
+/*
+ * erebus_b200.h -- C ABI of the B200-native marker-in-cell timestep library
+ * (liberebus_b200.so).
+ *
+ * The library replaces the per-timestep hot path of Erebus.jl (src/Erebus.jl,
+ * `simulation_loop` E:6370-7235) with device-resident state and hand-written
+ * sm_100a kernels.  Every entry point returns an int status (0 = OK, see
+ * EREBUS_E*); nothing throws and nothing aborts.  Host arrays stay owned by
+ * the caller; the library owns all device memory.  A state is not thread-safe.
+ *
+ * Array layouts are those of the reference: node arrays are column-major
+ * (Julia `Matrix{Float64}`), element (i,j) (1-based) at linear index
+ * (j-1)*rows + (i-1).  Basic-node arrays are (Ny, Nx); Vx, Vy and P arrays are
+ * all (Ny1, Nx1) with Ny1 = Ny+1, Nx1 = Nx+1 (src/Erebus.jl:173-277).  Bool
+ * arrays (YNY*) are one byte per element, as Julia's Array{Bool}.  Marker
+ * arrays are structure-of-arrays vectors of length >= marknum; the material
+ * type `tm` is Julia `Int` (int64).  Only square grids are supported
+ * (Nx == Ny, xsize == ysize), as in the reference, whose axis vectors are
+ * sized with the other dimension (src/constants.jl:47, :119).
+ */
+#ifndef EREBUS_B200_H
+#define EREBUS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define EREBUS_OK               0
+#define EREBUS_EINVAL           1   /* bad argument / parameter set */
+#define EREBUS_ECUDA            2   /* CUDA runtime error */
+#define EREBUS_ENOMEM           3   /* device allocation failed */
+#define EREBUS_ECAPACITY        4   /* marker capacity exceeded (replenish) */
+#define EREBUS_ENOCONV          5   /* a linear solve did not reach tolerance */
+#define EREBUS_ENONFINITE       6   /* NaN/Inf found where finite data is required */
+#define EREBUS_ENODEVICE        7   /* no CUDA device */
+
+/*
+ * Runtime parameter set: replaces the compile-time constants of
+ * src/constants.jl (C:1-447).  Material tables are indexed by marker type
+ * minus one (1 = mantle, 2 = crust, 3 = sticky air).  erebus_default_params()
+ * fills the values of src/constants.jl except for the grid, which callers set.
+ */
+typedef struct ErebusParams {
+    /* grid and geometry (C:6-33, C:104-106) */
+    int32_t Nx, Ny;            /* basic grid resolution; Nx1 = Nx+1 */
+    int32_t Nxmc, Nymc;        /* markers per cell in x and y */
+    double  xsize, ysize;      /* model size [m] */
+    double  rplanet, rcrust;   /* planet and crust radius [m] */
+    double  psurface;          /* surface pressure [Pa] */
+    /* material tables (C:146-186) */
+    double rhosolidm[3], rhofluidm[3], etasolidm[3], etasolidmm[3];
+    double etafluidm[3], etafluidmm[3], rhocpsolidm[3], rhocpfluidm[3];
+    double alphasolidm[3], alphafluidm[3], ksolidm[3], kfluidm[3];
+    double start_hrsolidm[3], start_hrfluidm[3], gggsolidm[3];
+    double frictsolidm[3], cohessolidm[3], tenssolidm[3];
+    double kphim0[3], tkm0[3], XWsolidm_init[3];
+    int32_t marker_property_mode;   /* 1: T-dependent laws, 9: constants (C:188) */
+    int32_t reaction_rate_coeff_mode;   /* 1, 2, 3 or 9 (C:271) */
+    double etaphikoef;               /* compaction viscosity coefficient (C:190) */
+    /* radiogenic heating (C:2-4, C:195-214) */
+    int32_t hr_al, hr_fe;
+    double t_half_al, ratio_al, E_al, f_al;
+    double t_half_fe, ratio_fe, E_fe, f_fe;
+    /* melting and porosity (C:216-229) */
+    double tmsolidphase, tmfluidphase, Lf;
+    double phim0, phimin, phimax;
+    /* thermodynamics of the dehydration reaction (C:230-281) */
+    double RG, MH2O, MD, rhoDs, rhoWs, rhoH2Of, rhoH2Ofi;
+    double dHWD, dSWD;
+    double pfcoeff, pferrmax;
+    int32_t reaction_active, _pad0;
+    double dtreaction, log_completion_rate;
+    double A_I, b_I, c_I, Sxo_B, Tscl_B, To_B, Sxo_T, To_T, Ea_T;
+    /* boundary conditions (C:283-310) */
+    double bcleft, bcright, bctop, bcbottom;
+    double bcfleft, bcfright, bcftop, bcfbottom;
+    double strainrate;         /* vxleft..vybottom derive from it (C:303-310) */
+    /* physics (C:137-143) */
+    double G, Kcont;
+    /* time stepping (C:311-366) */
+    double dt_longest, dtcoefdn, dtcoefup;
+    int32_t dtstep, nplast;
+    double dxymax, DTmax, dsubgridt, dsubgrids;
+    double start_time, endtime, etamin, etamax;
+    int32_t titermax, random_markers;
+    double yerrmax, etawt, dphimax;
+    uint64_t seed;
+    /* Extension with no reference counterpart: when non-zero, the solid
+       viscosity of rock markers comes from the per-marker array
+       `etasolidm_m` instead of the table `etasolidm[tm]` (workloads with a
+       log-uniform viscosity per marker).  0 = reference behaviour. */
+    int32_t per_marker_eta, _pad1;
+} ErebusParams;
+
+/*
+ * Host views of the marker SoA (src/Erebus.jl:426-552).  All pointers are
+ * caller-owned arrays of length >= the marker count in use.
+ */
+typedef struct ErebusMarkersHost {
+    double  *xm, *ym;
+    int64_t *tm;
+    double  *tkm, *sxxm, *sxym, *etavpm, *phim, *phinewm, *pfm0;
+    double  *XWsolidm, *XWsolidm0;
+    double  *rhototalm, *rhocptotalm, *etatotalm, *hrtotalm, *ktotalm;
+    double  *tkm_rhocptotalm, *etafluidcur_inv_kphim, *inv_gggtotalm;
+    double  *fricttotalm, *cohestotalm, *tenstotalm, *rhofluidcur;
+    double  *alphasolidcur, *alphafluidcur;
+    double  *etasolidm_m;      /* extension; NULL unless per_marker_eta */
+} ErebusMarkersHost;
+
+/*
+ * Host views of the staggered-grid state (src/Erebus.jl:147-415).  Basic
+ * arrays are (Ny,Nx); all others (Ny1,Nx1).  YNY, YNY5, YNY00 are bytes.
+ */
+typedef struct ErebusGridHost {
+    /* basic nodes */
+    double *ETA, *ETA0, *GGG, *EXY, *SXY, *SXY0, *wyx, *COH, *TEN, *FRI;
+    uint8_t *YNY;
+    double *ETA5, *ETA00;
+    uint8_t *YNY5, *YNY00;
+    double *YNY_inv_ETA, *DSXY, *DSY;
+    /* Vx nodes */
+    double *RHOX, *RHOFX, *KX, *PHIX, *vx, *vxf, *RX, *qxD, *gx;
+    /* Vy nodes */
+    double *RHOY, *RHOFY, *KY, *PHIY, *vy, *vyf, *RY, *qyD, *gy;
+    /* P nodes */
+    double *RHO, *RHOCP, *ALPHA, *ALPHAF, *HR, *HA, *HS, *ETAP, *GGGP;
+    double *EXX, *SXX, *SXX0, *tk1, *tk2, *DT, *DT0;
+    double *vxp, *vyp, *vxpf, *vypf, *pr, *pf, *ps, *pr0, *pf0, *ps0;
+    double *ETAPHI, *BETAPHI, *PHI, *APHI, *FI, *DMP, *DHP, *XWS;
+    double *EII, *SII, *DSXX, *tk0;
+} ErebusGridHost;
+
+/*
+ * Weighted sums of the marker->node scatter (src/Erebus.jl:851-923): the
+ * SUM arrays the reference keeps between phases.  Exported for parity tests.
+ * Basic (Ny,Nx): ETA0SUM..WTSUM; Vx/Vy/P (Ny1,Nx1): the rest.
+ */
+typedef struct ErebusSumsHost {
+    double *ETA0SUM, *ETASUM, *GGGSUM, *SXYSUM, *COHSUM, *TENSUM, *FRISUM, *WTSUM;
+    double *RHOXSUM, *RHOFXSUM, *KXSUM, *PHIXSUM, *RXSUM, *WTXSUM;
+    double *RHOYSUM, *RHOFYSUM, *KYSUM, *PHIYSUM, *RYSUM, *WTYSUM;
+    double *RHOSUM, *RHOCPSUM, *ALPHASUM, *ALPHAFSUM, *HRSUM, *GGGPSUM;
+    double *SXXSUM, *TKSUM, *PHISUM, *DMPSUM, *DHPSUM, *XWSSUM, *WTPSUM;
+} ErebusSumsHost;
+
+/* Per linear solve statistics. */
+typedef struct ErebusSolveStats {
+    int32_t iterations;        /* Krylov iterations (0 for a direct solve) */
+    int32_t converged;         /* 1 when the tolerance was met */
+    double  rel_residual;      /* ||b - A x|| / ||b|| at exit (scaled system) */
+} ErebusSolveStats;
+
+/* Per timestep statistics (what the reference logs, E:7217-7225). */
+typedef struct ErebusStepStats {
+    int32_t titer;             /* thermochemical iterations taken */
+    int32_t iplast_total;      /* plastic iterations summed over titer */
+    int32_t krylov_total;      /* Stokes-Darcy Krylov iterations summed */
+    int32_t thermal_total;     /* heat-equation Krylov iterations summed */
+    int32_t gravity_iters;     /* gravity Krylov iterations */
+    int32_t _pad;
+    int64_t marknum;           /* markers in use after replenishment */
+    double  dt;                /* timestep taken [s] */
+    double  timesum;           /* model time after the step [s] */
+    double  maxT;              /* max(tk2) [K] */
+    double  worst_rel_residual;/* worst final relative residual of any solve */
+} ErebusStepStats;
+
+/* Solver controls (the reference uses a direct LU, so these have no
+   counterpart; defaults come from erebus_default_solver_options). */
+typedef struct ErebusSolverOptions {
+    double  hydro_rtol;        /* Stokes-Darcy relative residual target */
+    double  thermal_rtol;      /* heat equation relative residual target */
+    double  gravity_rtol;      /* Poisson relative residual target */
+    int32_t max_iters;         /* Krylov iteration cap per solve */
+    int32_t restart;           /* GMRES restart length */
+} ErebusSolverOptions;
+
+typedef struct erebus_state erebus_state;
+
+/* ---- parameters --------------------------------------------------------- */
+/* Fills *p with the values of src/constants.jl (C:1-447) for the given
+   grid; derived quantities (dx, axes, marker grid) follow from the fields. */
+int erebus_default_params(ErebusParams *p, int32_t Nx, int32_t Ny);
+int erebus_default_solver_options(ErebusSolverOptions *o);
+/* Checks a parameter set (square grid, sizes, table values). */
+int erebus_check_params(const ErebusParams *p);
+
+/* ---- lifecycle (replaces the setup_* allocators E:55-592, E:851, E:2976) */
+int erebus_create(const ErebusParams *p, int64_t marker_capacity,
+                  erebus_state **out);
+int erebus_destroy(erebus_state *s);
+int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o);
+/* Last CUDA/solver error text for a state (NUL-terminated, owned by state). */
+const char *erebus_last_error(const erebus_state *s);
+
+/* ---- host <-> device ---------------------------------------------------- */
+int erebus_upload_markers(erebus_state *s, const ErebusMarkersHost *m,
+                          int64_t marknum);
+int erebus_download_markers(erebus_state *s, ErebusMarkersHost *m,
+                            int64_t *marknum);
+int erebus_upload_grid(erebus_state *s, const ErebusGridHost *g);
+int erebus_download_grid(erebus_state *s, ErebusGridHost *g);
+int erebus_download_sums(erebus_state *s, ErebusSumsHost *sums);
+/* dt / timesum / timestep counters of the device-side driver. */
+int erebus_set_time(erebus_state *s, double dt, double timesum);
+int erebus_get_time(const erebus_state *s, double *dt, double *timesum);
+
+/* ---- per-phase drop-ins (same semantics as the Julia functions) --------- */
+/* E:6376-6604: reset_interpolated_properties!, calculate_radioactive_heating,
+   compute_marker_properties! + marker_to_{basic,vx,vy,p}_nodes! over all
+   markers, compute_{basic,vx,vy,p}_node_properties!,
+   apply_insulating_boundary_conditions!(tk1). */
+int erebus_markers_to_nodes(erebus_state *s, double timesum);
+/* E:6610-6614: assemble_gravitational_lse!, LP\RP,
+   process_gravitational_solution! */
+int erebus_gravity(erebus_state *s, ErebusSolveStats *st);
+/* E:2558-2694: perform_thermochemical_reaction! */
+int erebus_thermochemical_reaction(erebus_state *s, double dt, int32_t timestep,
+                                   int32_t titer);
+/* E:6678-6869: one plastic pass: recompute_bulk_viscosity!,
+   assemble_hydromechanical_lse! + solve, process_hydromechanical_solution!,
+   compute_Aphi!, compute_fluid_velocities!, compute_displacement_timestep,
+   compute_stress_strainrate!, compute_Aphi!, symmetrize_p_node_observables!,
+   compute_nodal_adjustment! and (when not converged)
+   finalize_plastic_iteration_pass!.  *dt is updated; *converged receives the
+   value compute_nodal_adjustment! returns. */
+int erebus_hydromech_pass(erebus_state *s, double *dt, int32_t iplast,
+                          int32_t *converged, ErebusSolveStats *st);
+/* E:6887-6927: compute_shear_heating!, (timestep==1 pressure copy),
+   compute_adiabatic_heating!, assemble_thermal_lse! + solve, DT = tk2-tk1.
+   Returns max|DT| in *maxDT. */
+int erebus_thermal_solve(erebus_state *s, double dt, int32_t timestep,
+                         double *maxDT, ErebusSolveStats *st);
+/* E:6945-7019: DT0 copy, update_marker_viscosity!, update_marker_stress!,
+   update_marker_temperature!, XWsolidm0/phim copies, update_marker_porosity!,
+   update_p_nodes_melt_composition! */
+int erebus_nodes_to_markers(erebus_state *s, double dt, int32_t timestep);
+/* E:7026-7059: compute_velocities!, compute_rotation_rate!,
+   move_markers_rk4!, backtrace_pressures_rk4! */
+int erebus_advect_rk4(erebus_state *s, double dt);
+/* E:7065: replenish_markers!; *marknum receives the new count.
+   EREBUS_ECAPACITY when the marker capacity would be exceeded. */
+int erebus_replenish(erebus_state *s, int32_t timestep, int64_t *marknum);
+/* E:6370-7235: one whole timestep (all of the above in reference order,
+   with the thermochemical and plastic iteration loops).  Updates the
+   state's dt and timesum. */
+int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st);
+
+/* ---- debugging / parity ----------------------------------------------- */
+/* Assembles the Stokes-Darcy system of E:3089-3572 from the current device
+   state and copies it out in CSC form (0-based, the reference's row order).
+   nnz_out receives the entry count; pass colptr/rowval/nzval = NULL to query
+   it.  R receives the right-hand side (6*Ny1*Nx1). */
+int erebus_export_hydromech(erebus_state *s, double dt, int64_t *nnz_out,
+                            int64_t *colptr, int64_t *rowval, double *nzval,
+                            double *R);
+/* Applies the device Stokes-Darcy operator y = L x (matrix-free, same
+   coefficients as the assembled matrix). */
+int erebus_apply_hydromech(erebus_state *s, double dt, const double *x,
+                           double *y);
+/* Number of kernel launches issued by this state since creation. */
+int erebus_kernel_launches(const erebus_state *s, int64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EREBUS_B200_H */
