@@ -1,0 +1,337 @@
+"""Benchmark: MIC timesteps per second of the plain FP64 GPU path.
+
+Workload: the synthetic 141x141 planetesimal (490,000 markers, 5x5 per
+cell; 140 km box, 50 km rock body in sticky air; per-marker porosity
+U(0.05, 0.25) and log-uniform rock viscosity 1e18-1e20 Pa s).  A step is one
+whole timestep of simulation_loop (src/Erebus.jl:6370-7235).  With N GPUs
+(torchrun) every rank advances its own planetesimal (replicas; the path has
+no exchange step) and `value` is all ranks' timesteps over the slowest
+rank's device time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "MIC timesteps/sec (plain FP64 GPU path)"
+UNIT = "timesteps/s"
+WORKLOAD = "planetesimal_141"
+
+
+def load_pkg():
+    import importlib.util
+    if "erebus_b200" in sys.modules:
+        return sys.modules["erebus_b200"]
+    pkg_dir = os.path.join(ROOT, "erebus.jl_b200")
+    spec = importlib.util.spec_from_file_location(
+        "erebus_b200", os.path.join(pkg_dir, "__init__.py"),
+        submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["erebus_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    return O
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def config_dict(pkg, name, extra=None):
+    c = pkg.CONFIGS[name]
+    d = {"workload": name, "grid": "%dx%d basic nodes" % (c["N"], c["N"]),
+         "markers_per_cell": "%dx%d" % (c["mpc"], c["mpc"]),
+         "l2": "inputs larger than L2 (band LU storage ~1.9 GB, 490k-marker SoA ~110 MB "
+               "streamed every step)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), "--query-gpu=" + q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() in ("active", "1"):
+                        reasons.add(nm)
+            except Exception:
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def pin_host_state(st):
+    """Moves the HostState arrays into pinned host memory."""
+    import torch
+    for d in (st.m, st.grid):
+        for k, a in list(d.items()):
+            t = torch.empty(a.size, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+            v = t.numpy().reshape(a.shape, order="F" if a.ndim > 1 else "C")
+            v[...] = a
+            d[k] = v
+    return st
+
+
+def cpu_baseline(pkg, O, name, steps=2):
+    """The oracle (C restatement + SuperLU) on the host cores: timestep 1
+    untimed, then `steps` timesteps timed."""
+    st = pkg.make_state(name)
+    o = O.Oracle(st)
+    o.step(1)
+    t0 = time.perf_counter()
+    for ts in range(2, 2 + steps):
+        o.step(ts)
+    el = time.perf_counter() - t0
+    return {"value": steps / el, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": "%s timesteps 2-%d of the same workload (timestep 1 untimed): OpenMP "
+                      "on the marker loops the reference threads, SuperLU direct solves, "
+                      "%.1f s" % (name, 1 + steps, el)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pkg = load_pkg()
+    O = load_oracle()
+    st = pkg.make_state(WORKLOAD)
+    o = O.Oracle(st)
+    for ts in range(1, args.warmup + 1):
+        o.step(ts)
+    t0 = time.perf_counter()
+    for ts in range(args.warmup + 1, args.warmup + args.steps + 1):
+        o.step(ts)
+    el = time.perf_counter() - t0
+    v = args.steps / el
+    cores = os.cpu_count()
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(pkg, WORKLOAD),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "timesteps %d-%d after %d untimed, oracle restatement "
+                                       "of the reference (Julia is not available) with "
+                                       "SuperLU solves" % (args.warmup + 1,
+                                                           args.warmup + args.steps,
+                                                           args.warmup)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def algorithmic_bytes(sim, st):
+    """Bytes each phase must move once (per launch of the phase)."""
+    g = st.g
+    n = st.marknum
+    nodes = g.Nx1 * g.Ny1
+    tiles = lambda sysn: sysn  # placeholder for clarity
+    nbt = 64
+    NBh = (6 * nodes + nbt - 1) // nbt
+    Bbh = (6 * g.Ny1 + 2 + nbt - 1) // nbt
+    band_h = NBh * (2 * Bbh + 1) * nbt * nbt * 8
+    return {
+        # read 16 marker fields (129 B) + write 7 derived (56 B); ~217 B per
+        # P node of normalised outputs
+        "markers_to_nodes": 185 * n + 217 * nodes,
+        "rk4": 97 * n,
+        "nodes_to_markers": 137 * n,
+        "reaction": 73 * n,
+        # the band is read and written once by the factorisation
+        "hydro_factor": 2 * band_h,
+        "hydro_solve": band_h,
+    }
+
+
+def run_ours(args):
+    rank, world, local = dist_setup(args.gpus)
+    import torch
+    pkg = load_pkg()
+    st = pkg.make_state(WORKLOAD)
+    sim = pkg.Simulation(st)
+    for ts in range(1, args.warmup + 1):
+        sim.step(ts)
+    sim.enable_phase_timing(True)
+    l0 = sim.kernel_launches()
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local) if rank == 0 else None
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    stats = []
+    for ts in range(args.warmup + 1, args.warmup + args.steps + 1):
+        stats.append(sim.step(ts))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ck = clocks.stop() if clocks else None
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, world)
+    launches = sim.kernel_launches() - l0
+    phases = sim.phase_times()
+    value = world * args.steps / (ms_max / 1000.0)
+
+    # end to end through the public API: host buffers (pinned) uploaded,
+    # one timestep, results downloaded, every step
+    st2 = pin_host_state(pkg.make_state(WORKLOAD))
+    sim.close()
+    sim2 = pkg.Simulation(st2)
+    for ts in range(1, 3):
+        sim2.step(ts)
+    sim2.download()
+    h2d = sum(a[: st2.marknum].nbytes for k, a in st2.m.items() if k != "etasolidm_m") + \
+        sum(a.nbytes for a in st2.grid.values())
+    if st2.p.per_marker_eta:
+        h2d += st2.m["etasolidm_m"][: st2.marknum].nbytes
+    d2h = h2d
+    stream2 = torch.cuda.ExternalStream(sim2.stream_handle())
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ne2e = max(2, min(args.steps, 3))
+    barrier(world)
+    torch.cuda.synchronize()
+    e2.record(stream2)
+    for ts in range(3, 3 + ne2e):
+        sim2.upload()
+        sim2.step(ts)
+        sim2.download()
+    e3.record(stream2)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
+    sim2.close()
+    e2e = {"value": world * ne2e / (e2e_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+           "steps": ne2e}
+
+    if rank == 0:
+        hbm, src = peaks()
+        ab = algorithmic_bytes(None, st)
+        per = {}
+        for k, (t, c) in phases.items():
+            if c:
+                ent = {"ms_total": round(t, 3), "launches": c, "ms_per_launch": t / c}
+                if k in ab:
+                    ent["GBps"] = ab[k] / (t / c / 1000.0) / 1e9
+                per[k] = ent
+        dom = max(per, key=lambda k: per[k]["ms_total"])
+        roof = None
+        hbm_dom = dom if dom in ab else max((k for k in per if k in ab),
+                                            key=lambda k: per[k]["ms_total"])
+        a = per[hbm_dom]["GBps"]
+        roof = {"bound": "hbm", "kernel": hbm_dom, "achieved": a, "peak": hbm, "unit": "GB/s",
+                "frac": a / hbm, "peak_source": src, "traffic": None,
+                "bytes_per_launch": ab[hbm_dom],
+                "note": "dominant phase by device time: %s" % dom}
+        cpu = None if args.no_cpu_baseline else cpu_baseline(pkg, load_oracle(), WORKLOAD)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config_dict(pkg, WORKLOAD,
+                                      {"parallelism": "replicas x%d" % world,
+                                       "titer_per_step": [s.titer for s in stats],
+                                       "factorizations": [s.factorizations for s in stats]}),
+                "roofline": roof, "phases": per, "cpu_baseline": cpu, "clocks": ck,
+                "e2e": e2e, "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

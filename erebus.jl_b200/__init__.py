@@ -11,3 +11,5 @@ from .abi import (ErebusGridHost, ErebusMarkersHost, ErebusParams,  # noqa: F401
 from .host import (Geometry, HostState, define_markers, make_state,  # noqa: F401
                    u01)
 from .params import CONFIGS, config_params, default_params  # noqa: F401
+from .device import (ErebusError, Simulation, load_library,  # noqa: F401,E402
+                     run_simulation)

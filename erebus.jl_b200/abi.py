@@ -146,7 +146,7 @@ class ErebusSolveStats(Structure):
 class ErebusStepStats(Structure):
     _fields_ = [
         ("titer", c_int32), ("iplast_total", c_int32), ("krylov_total", c_int32),
-        ("thermal_total", c_int32), ("gravity_iters", c_int32), ("_pad", c_int32),
+        ("thermal_total", c_int32), ("gravity_iters", c_int32), ("factorizations", c_int32),
         ("marknum", c_int64), ("dt", c_double), ("timesum", c_double),
         ("maxT", c_double), ("worst_rel_residual", c_double),
     ]

@@ -1,0 +1,683 @@
+// api.cu -- the extern "C" boundary of liberebus_b200.so (include/erebus_b200.h)
+// and the host-side timestep driver.
+//
+// The driver follows simulation_loop (src/Erebus.jl:6370-7235): every phase
+// is enqueued on the state's stream; the host waits only where the
+// reference makes a decision (plastic and thermochemical convergence, the
+// dt updates, the new marker count).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include "stencils.cuh"
+
+using namespace erebus;
+
+namespace erebus {
+int check_cuda(erebus_state *s, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return EREBUS_OK;
+    if (s) s->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? EREBUS_ENOMEM : EREBUS_ECUDA;
+}
+
+static cudaEvent_t timer_event(erebus_state *s) {
+    if (!s->ev_pool.empty()) {
+        cudaEvent_t e = s->ev_pool.back();
+        s->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void timer_begin(erebus_state *s, int phase) {
+    if (!s->timing || phase < 0 || phase >= 32) return;
+    cudaEvent_t e = timer_event(s);
+    cudaEventRecord(e, s->stream);
+    s->ev_open[phase] = e;
+}
+
+void timer_end(erebus_state *s, int phase) {
+    if (!s->timing || phase < 0 || phase >= 32 || !s->ev_open[phase]) return;
+    cudaEvent_t e = timer_event(s);
+    cudaEventRecord(e, s->stream);
+    s->ev_pending.push_back({phase, {s->ev_open[phase], e}});
+    s->ev_open[phase] = nullptr;
+}
+
+void timer_collect(erebus_state *s) {
+    for (auto &p : s->ev_pending) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) {
+            s->phase_ms[p.first] += ms;
+            s->phase_count[p.first] += 1;
+        }
+        s->ev_pool.push_back(p.second.first);
+        s->ev_pool.push_back(p.second.second);
+    }
+    s->ev_pending.clear();
+}
+}  // namespace erebus
+
+#define TRY(x)                   \
+    do {                         \
+        int _rc = (x);           \
+        if (_rc) return _rc;     \
+    } while (0)
+
+static bool is_basic_field(int f) { return f < G_FIRST_P; }
+static bool is_bool_field(int f) { return f == G_YNY || f == G_YNY5 || f == G_YNY00; }
+static bool is_basic_sum(int f) { return f < S_FIRST_P; }
+
+static void set3(double *a, double x, double y, double z) {
+    a[0] = x;
+    a[1] = y;
+    a[2] = z;
+}
+
+extern "C" {
+
+// src/constants.jl (C:1-447)
+int erebus_default_params(ErebusParams *p, int32_t Nx, int32_t Ny) {
+    if (!p) return EREBUS_EINVAL;
+    std::memset(p, 0, sizeof(*p));
+    p->Nx = Nx;
+    p->Ny = Ny;
+    p->Nxmc = p->Nymc = 4;
+    p->xsize = p->ysize = 14000.0;
+    p->rplanet = 5000.0;
+    p->rcrust = 4800.0;
+    p->psurface = 1.0e3;
+    set3(p->rhosolidm, 3300.0, 3300.0, 1.0);
+    set3(p->rhofluidm, 1000.0, 1000.0, 1.0);
+    set3(p->etasolidm, 1e19, 1e19, 1e16);
+    set3(p->etasolidmm, 1e19, 1e19, 1e16);
+    set3(p->etafluidm, 1e12, 1e12, 1e-3);
+    set3(p->etafluidmm, 1e-3, 1e-3, 1e-3);
+    set3(p->rhocpsolidm, 3.3e6, 3.3e6, 3.0e6);
+    set3(p->rhocpfluidm, 1.0e6, 1.0e6, 3.0e6);
+    set3(p->alphasolidm, 3.0e-5, 3.0e-5, 0.0);
+    set3(p->alphafluidm, 5.0e-5, 5.0e-5, 0.0);
+    set3(p->ksolidm, 3.0, 3.0, 3000.0);
+    set3(p->kfluidm, 50.0, 50.0, 3000.0);
+    set3(p->start_hrsolidm, 0.0, 0.0, 0.0);
+    set3(p->start_hrfluidm, 0.0, 0.0, 0.0);
+    set3(p->gggsolidm, 1e10, 1e10, 1e10);
+    set3(p->frictsolidm, 0.6, 0.6, 0.0);
+    set3(p->cohessolidm, 1e8, 1e8, 1e8);
+    set3(p->tenssolidm, 6e7, 6e7, 6e7);
+    set3(p->kphim0, 1e-13, 1e-13, 1e-17);
+    set3(p->tkm0, 170.0, 170.0, 170.0);
+    set3(p->XWsolidm_init, 0.5, 0.5, NAN);
+    p->marker_property_mode = 9;
+    p->reaction_rate_coeff_mode = 1;
+    p->etaphikoef = 1.0;
+    p->hr_al = 1;
+    p->hr_fe = 0;
+    p->t_half_al = 717000.0 * 31540000.0;
+    p->ratio_al = 5.0e-5;
+    p->E_al = 5.0470e-13;
+    p->f_al = 1.9e23;
+    p->t_half_fe = 2620000.0 * 31540000.0;
+    p->ratio_fe = 1.0e-6;
+    p->E_fe = 4.34e-13;
+    p->f_fe = 1.957e24;
+    p->tmsolidphase = 1416.0;
+    p->tmfluidphase = 273.0;
+    p->Lf = 333.55e3;
+    p->phim0 = 0.2;
+    p->phimin = 1.0e-4;
+    p->phimax = 1.0 - p->phimin;
+    p->RG = 8.314;
+    p->MH2O = 0.018;
+    p->MD = 0.120;
+    p->rhoDs = 3300.0;
+    p->rhoWs = 2600.0;
+    p->rhoH2Of = 1000.0;
+    p->rhoH2Ofi = 917.0;
+    p->dHWD = 40000.0;
+    p->dSWD = 60.0;
+    p->pfcoeff = 0.5;
+    p->pferrmax = 1.0e5;
+    p->reaction_active = 1;
+    p->dtreaction = 1.0e10;
+    p->log_completion_rate = std::log(0.01);
+    p->A_I = 1.0e-11;
+    p->b_I = 2.5e-4;
+    p->c_I = 543.0;
+    p->Sxo_B = 2.0e-11;
+    p->Tscl_B = 10.0;
+    p->To_B = 293.0;
+    p->Sxo_T = 2.0e-11;
+    p->To_T = 293.0;
+    p->Ea_T = 63.8e3;
+    p->bcleft = p->bcright = p->bctop = p->bcbottom = -1.0;
+    p->bcfleft = p->bcfright = p->bcftop = p->bcfbottom = -1.0;
+    p->strainrate = 0.0;
+    p->G = 6.672e-11;
+    p->Kcont = 1.0e20;
+    p->dt_longest = 1.0e11;
+    p->dtcoefdn = 0.5;
+    p->dtcoefup = 1.2;
+    p->dtstep = 200;
+    p->nplast = 100000;
+    p->dxymax = 0.05;
+    p->DTmax = 20.0;
+    p->dsubgridt = p->dsubgrids = 0.0;
+    const double yearlength = 365.25 * 24 * 3600;
+    p->start_time = 2.25e6 * yearlength;
+    p->endtime = 15.0e6 * yearlength;
+    p->etamin = 1e12;
+    p->etamax = 1e23;
+    p->titermax = 10000;
+    p->random_markers = 1;
+    p->yerrmax = 1e2;
+    p->etawt = 0.0;
+    p->dphimax = 100.01;
+    p->seed = 42;
+    p->per_marker_eta = 0;
+    return EREBUS_OK;
+}
+
+int erebus_default_solver_options(ErebusSolverOptions *o) {
+    if (!o) return EREBUS_EINVAL;
+    o->hydro_rtol = 1e-13;
+    o->thermal_rtol = 1e-13;
+    o->gravity_rtol = 1e-13;
+    o->max_iters = 4;
+    o->restart = 0;
+    return EREBUS_OK;
+}
+
+int erebus_check_params(const ErebusParams *p) {
+    if (!p) return EREBUS_EINVAL;
+    if (p->Nx < 4 || p->Ny < 4 || p->Nx != p->Ny) return EREBUS_EINVAL;
+    if (!(p->xsize > 0) || p->xsize != p->ysize) return EREBUS_EINVAL;
+    if (p->Nxmc < 1 || p->Nymc < 1) return EREBUS_EINVAL;
+    if (p->marker_property_mode != 1 && p->marker_property_mode != 9) return EREBUS_EINVAL;
+    int rm = p->reaction_rate_coeff_mode;
+    if (rm != 1 && rm != 2 && rm != 3 && rm != 9) return EREBUS_EINVAL;
+    if (p->dtstep < 1 || p->titermax < 1 || p->nplast < 1) return EREBUS_EINVAL;
+    if (p->dsubgridt != 0.0 || p->dsubgrids != 0.0) return EREBUS_EINVAL;
+    return EREBUS_OK;
+}
+
+const char *erebus_last_error(const erebus_state *s) {
+    return s ? s->last_error.c_str() : "null state";
+}
+
+int erebus_destroy(erebus_state *s) {
+    if (!s) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (void *p : s->allocations) cudaFree(p);
+    band_free(s->hydro);
+    band_free(s->thermal);
+    band_free(s->gravity);
+    if (s->hsc) cudaFreeHost(s->hsc);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return EREBUS_OK;
+}
+
+int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state **out) {
+    if (!p || !out || marker_capacity < 1 || marker_capacity > (int64_t)1 << 30)
+        return EREBUS_EINVAL;
+    *out = nullptr;
+    int rc = erebus_check_params(p);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return EREBUS_ENODEVICE;
+    erebus_state *s = new erebus_state();
+    s->p = *p;
+    erebus_default_solver_options(&s->opt);
+    s->g = make_geo(*p);
+    s->capacity = marker_capacity;
+    s->dt = p->dt_longest;
+    s->timesum = p->start_time;
+    cudaGetDevice(&s->device);
+    auto fail = [&](int code, const char *what) {
+        s->last_error = std::string("erebus_create: ") + what;
+        erebus_destroy(s);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(EREBUS_ECUDA, "stream");
+    auto alloc = [&](size_t bytes) -> void * {
+        void *ptr = nullptr;
+        if (cudaMalloc(&ptr, bytes) != cudaSuccess) return nullptr;
+        cudaMemset(ptr, 0, bytes);
+        s->allocations.push_back(ptr);
+        return ptr;
+    };
+    const Geo &g = s->g;
+    size_t cap = (size_t)marker_capacity;
+    size_t np = (size_t)g.Nx1 * g.Ny1, nbn = (size_t)g.Nx * g.Ny;
+    for (int f = 0; f < M_COUNT; f++) {
+        if (f == M_tm) continue;
+        s->m[f] = (double *)alloc(cap * 8);
+        if (!s->m[f]) return fail(EREBUS_ENOMEM, "markers");
+    }
+    s->tm8 = (int8_t *)alloc(cap);
+    if (!s->tm8) return fail(EREBUS_ENOMEM, "markers");
+    for (int f = 0; f < G_COUNT; f++) {
+        size_t n = is_basic_field(f) ? nbn : np;
+        s->grid[f] = (double *)alloc(is_bool_field(f) ? n : n * 8);
+        if (!s->grid[f]) return fail(EREBUS_ENOMEM, "grid");
+    }
+    for (int f = 0; f < S_COUNT; f++) {
+        s->sums[f] = (double *)alloc((is_basic_sum(f) ? nbn : np) * 8);
+        if (!s->sums[f]) return fail(EREBUS_ENOMEM, "sums");
+    }
+    for (int gr = 0; gr < 4; gr++) {
+        GridSpec sp = grid_spec(g, gr);
+        CellSort &cs = s->sort[gr];
+        cs.ncells = sp.rows * sp.cols;
+        cs.count = (int *)alloc((cs.ncells + 1) * 4);
+        cs.cursor = (int *)alloc((cs.ncells + 1) * 4);
+        cs.start = (int *)alloc((cs.ncells + 1) * 4);
+        cs.idx = (int *)alloc(cap * 4);
+        cs.tmp = (int *)alloc(cap * 4);
+        if (!cs.count || !cs.cursor || !cs.start || !cs.idx || !cs.tmp)
+            return fail(EREBUS_ENOMEM, "sort");
+    }
+    s->r_dM = (double *)alloc(cap * 8);
+    s->r_dH = (double *)alloc(cap * 8);
+    s->r_flag = (int8_t *)alloc(cap);
+    s->tmp_node = (double *)alloc(2 * np * 8);
+    size_t na = (size_t)g.Nxm * g.Nym;
+    s->a_mdis = (unsigned long long *)alloc(na * 8);
+    s->a_mnum = (int *)alloc(na * 4);
+    s->a_src = (int *)alloc(na * 4);
+    s->a_rank = (int *)alloc(na * 4);
+    s->a_flag = (int *)alloc(na * 4);
+    s->dsc = (DevScalars *)alloc(sizeof(DevScalars));
+    if (!s->r_dM || !s->r_dH || !s->r_flag || !s->tmp_node || !s->a_mdis || !s->a_mnum ||
+        !s->a_src || !s->a_rank || !s->a_flag || !s->dsc)
+        return fail(EREBUS_ENOMEM, "scratch");
+    if (cudaMallocHost(&s->hsc, sizeof(DevScalars)) != cudaSuccess)
+        return fail(EREBUS_ENOMEM, "pinned scalars");
+    std::memset(s->hsc, 0, sizeof(DevScalars));
+    if (band_alloc(s, s->hydro, 6 * (int64_t)np, 6 * g.Ny1 + 2, 64, 12))
+        return fail(EREBUS_ENOMEM, "hydro system");
+    if (band_alloc(s, s->thermal, (int64_t)np, g.Ny1, 64, 5))
+        return fail(EREBUS_ENOMEM, "thermal system");
+    if (band_alloc(s, s->gravity, (int64_t)np, g.Ny1, 64, 5))
+        return fail(EREBUS_ENOMEM, "gravity system");
+    s->hydro.ph_factor = PH_HYDRO_FACTOR;
+    s->hydro.ph_solve = PH_HYDRO_SOLVE;
+    s->thermal.ph_factor = PH_THERMAL_FACTOR;
+    s->thermal.ph_solve = PH_THERMAL_SOLVE;
+    if (cudaDeviceSynchronize() != cudaSuccess) return fail(EREBUS_ECUDA, "init");
+    *out = s;
+    return EREBUS_OK;
+}
+
+int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o) {
+    if (!s || !o) return EREBUS_EINVAL;
+    s->opt = *o;
+    s->opt_no_reuse = o->restart < 0;
+    return EREBUS_OK;
+}
+
+// ---- host <-> device --------------------------------------------------------
+int erebus_upload_markers(erebus_state *s, const ErebusMarkersHost *m, int64_t marknum) {
+    if (!s || !m || marknum < 0 || marknum > s->capacity) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    const void *const *src = reinterpret_cast<const void *const *>(m);
+    for (int f = 0; f < M_COUNT; f++) {
+        if (f == M_tm) continue;
+        if (!src[f]) {
+            if (f == M_etasolidm_m && !s->p.per_marker_eta) continue;
+            return EREBUS_EINVAL;
+        }
+        TRY(check_cuda(s, cudaMemcpyAsync(s->m[f], src[f], marknum * 8,
+                                          cudaMemcpyHostToDevice, s->stream), "upload"));
+    }
+    std::vector<int8_t> t(marknum);
+    for (int64_t k = 0; k < marknum; k++) {
+        int64_t v = m->tm[k];
+        if (v < 1 || v > 3) return EREBUS_EINVAL;
+        t[k] = (int8_t)v;
+    }
+    TRY(check_cuda(s, cudaMemcpyAsync(s->tm8, t.data(), marknum, cudaMemcpyHostToDevice,
+                                      s->stream), "upload tm"));
+    TRY(check_cuda(s, cudaStreamSynchronize(s->stream), "upload"));
+    s->marknum = marknum;
+    s->sorted_valid = false;
+    return EREBUS_OK;
+}
+
+int erebus_download_markers(erebus_state *s, ErebusMarkersHost *m, int64_t *marknum) {
+    if (!s || !m) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    int64_t n = s->marknum;
+    void **dst = reinterpret_cast<void **>(m);
+    for (int f = 0; f < M_COUNT; f++) {
+        if (f == M_tm || !dst[f]) continue;
+        TRY(check_cuda(s, cudaMemcpyAsync(dst[f], s->m[f], n * 8, cudaMemcpyDeviceToHost,
+                                          s->stream), "download"));
+    }
+    std::vector<int8_t> t(n);
+    TRY(check_cuda(s, cudaMemcpyAsync(t.data(), s->tm8, n, cudaMemcpyDeviceToHost, s->stream),
+                   "download tm"));
+    TRY(check_cuda(s, cudaStreamSynchronize(s->stream), "download"));
+    if (m->tm)
+        for (int64_t k = 0; k < n; k++) m->tm[k] = t[k];
+    if (marknum) *marknum = n;
+    return EREBUS_OK;
+}
+
+static size_t field_bytes(erebus_state *s, int f) {
+    size_t n = is_basic_field(f) ? (size_t)s->g.Nx * s->g.Ny : (size_t)s->g.Nx1 * s->g.Ny1;
+    return is_bool_field(f) ? n : n * 8;
+}
+
+int erebus_upload_grid(erebus_state *s, const ErebusGridHost *gh) {
+    if (!s || !gh) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    const void *const *src = reinterpret_cast<const void *const *>(gh);
+    for (int f = 0; f < G_COUNT; f++) {
+        if (!src[f]) return EREBUS_EINVAL;
+        TRY(check_cuda(s, cudaMemcpyAsync(s->grid[f], src[f], field_bytes(s, f),
+                                          cudaMemcpyHostToDevice, s->stream), "upload grid"));
+    }
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "upload grid");
+}
+
+int erebus_download_grid(erebus_state *s, ErebusGridHost *gh) {
+    if (!s || !gh) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    void **dst = reinterpret_cast<void **>(gh);
+    for (int f = 0; f < G_COUNT; f++) {
+        if (!dst[f]) continue;
+        TRY(check_cuda(s, cudaMemcpyAsync(dst[f], s->grid[f], field_bytes(s, f),
+                                          cudaMemcpyDeviceToHost, s->stream), "download grid"));
+    }
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "download grid");
+}
+
+int erebus_download_sums(erebus_state *s, ErebusSumsHost *sh) {
+    if (!s || !sh) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    void **dst = reinterpret_cast<void **>(sh);
+    for (int f = 0; f < S_COUNT; f++) {
+        if (!dst[f]) continue;
+        size_t n = is_basic_sum(f) ? (size_t)s->g.Nx * s->g.Ny : (size_t)s->g.Nx1 * s->g.Ny1;
+        TRY(check_cuda(s, cudaMemcpyAsync(dst[f], s->sums[f], n * 8, cudaMemcpyDeviceToHost,
+                                          s->stream), "download sums"));
+    }
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "download sums");
+}
+
+int erebus_set_time(erebus_state *s, double dt, double timesum) {
+    if (!s) return EREBUS_EINVAL;
+    s->dt = dt;
+    s->timesum = timesum;
+    return EREBUS_OK;
+}
+
+int erebus_get_time(const erebus_state *s, double *dt, double *timesum) {
+    if (!s) return EREBUS_EINVAL;
+    if (dt) *dt = s->dt;
+    if (timesum) *timesum = s->timesum;
+    return EREBUS_OK;
+}
+
+int erebus_kernel_launches(const erebus_state *s, int64_t *count) {
+    if (!s || !count) return EREBUS_EINVAL;
+    *count = s->launches;
+    return EREBUS_OK;
+}
+
+int erebus_get_stream(const erebus_state *s, void **stream) {
+    if (!s || !stream) return EREBUS_EINVAL;
+    *stream = (void *)s->stream;
+    return EREBUS_OK;
+}
+
+int erebus_enable_phase_timing(erebus_state *s, int32_t on) {
+    if (!s) return EREBUS_EINVAL;
+    cudaStreamSynchronize(s->stream);
+    timer_collect(s);
+    s->timing = on != 0;
+    for (int k = 0; k < 32; k++) {
+        s->phase_ms[k] = 0.0;
+        s->phase_count[k] = 0;
+    }
+    return EREBUS_OK;
+}
+
+int erebus_phase_times(erebus_state *s, double *ms, int64_t *counts, int32_t n) {
+    if (!s || !ms || !counts || n < 1) return EREBUS_EINVAL;
+    cudaStreamSynchronize(s->stream);
+    timer_collect(s);
+    for (int k = 0; k < n && k < 32; k++) {
+        ms[k] = s->phase_ms[k];
+        counts[k] = s->phase_count[k];
+    }
+    return EREBUS_OK;
+}
+
+}  // extern "C"
+
+// ---- phases -----------------------------------------------------------------
+static int set_dev_dt(erebus_state *s, double dt) {
+    s->hsc->dt = dt;
+    return check_cuda(s, cudaMemcpyAsync(&s->dsc->dt, &s->hsc->dt, sizeof(double),
+                                         cudaMemcpyHostToDevice, s->stream), "dt");
+}
+
+static int read_scalars(erebus_state *s) {
+    TRY(check_cuda(s, cudaMemcpyAsync(s->hsc, s->dsc, sizeof(DevScalars),
+                                      cudaMemcpyDeviceToHost, s->stream), "scalars"));
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "scalars");
+}
+
+static double slot(const erebus_state *s, int k) { return s->hsc->maxabs[k]; }
+
+extern "C" {
+
+int erebus_markers_to_nodes(erebus_state *s, double timesum) {
+    if (!s) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    TRY(markers_to_nodes(s, timesum));
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "markers_to_nodes");
+}
+
+int erebus_gravity(erebus_state *s, ErebusSolveStats *st) {
+    if (!s) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    TRY(assemble_system(s, SYS_GRAVITY));
+    TRY(band_solve_refined(s, s->gravity, s->opt.gravity_rtol, s->opt.max_iters, st));
+    size_t np = (size_t)s->g.Nx1 * s->g.Ny1;
+    TRY(check_cuda(s, cudaMemcpyAsync(s->grid[G_FI], s->gravity.x, np * 8,
+                                      cudaMemcpyDeviceToDevice, s->stream), "FI"));
+    TRY(gravity_post(s));
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "gravity");
+}
+
+int erebus_thermochemical_reaction(erebus_state *s, double dt, int32_t timestep,
+                                   int32_t titer) {
+    if (!s) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    TRY(thermochemical_reaction(s, dt, timestep, titer));
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "reaction");
+}
+
+int erebus_hydromech_pass(erebus_state *s, double *dt, int32_t iplast, int32_t *converged,
+                          ErebusSolveStats *st) {
+    if (!s || !dt) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    TRY(set_dev_dt(s, *dt));
+    timer_begin(s, PH_HYDRO_ASSEMBLE);
+    TRY(bulk_viscosity(s));
+    TRY(assemble_system(s, SYS_HYDRO));
+    timer_end(s, PH_HYDRO_ASSEMBLE);
+    TRY(band_solve_refined(s, s->hydro, s->opt.hydro_rtol, s->opt.max_iters, st));
+    timer_begin(s, PH_HYDRO_POST);
+    TRY(hydro_post(s, s->hydro.x));
+    timer_end(s, PH_HYDRO_POST);
+    TRY(read_scalars(s));
+    double d = s->hsc->dt;
+    int ynpl = s->hsc->ynpl;
+    double yerr = ynpl > 0 ? std::sqrt(s->hsc->sum_ddd / ynpl) : 0.0;
+    int conv = ynpl == 0 || yerr < s->p.yerrmax || iplast == s->p.nplast;
+    if (!conv) {
+        int rollback = iplast % s->p.dtstep == 0;
+        if (rollback) d *= s->p.dtcoefdn;
+        TRY(finalize_plastic(s, rollback));
+        TRY(set_dev_dt(s, d));
+    }
+    *dt = d;
+    if (converged) *converged = conv;
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "hydromech_pass");
+}
+
+int erebus_thermal_solve(erebus_state *s, double dt, int32_t timestep, double *maxDT,
+                         ErebusSolveStats *st) {
+    if (!s) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    TRY(heating(s));
+    if (timestep == 1) {
+        size_t np = (size_t)s->g.Nx1 * s->g.Ny1 * 8;
+        cudaMemcpyAsync(s->grid[G_pr0], s->grid[G_pr], np, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(s->grid[G_pf0], s->grid[G_pf], np, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(s->grid[G_ps0], s->grid[G_ps], np, cudaMemcpyDeviceToDevice, s->stream);
+    }
+    TRY(adiabatic(s));
+    TRY(set_dev_dt(s, dt));
+    timer_begin(s, PH_THERMAL_ASSEMBLE);
+    TRY(assemble_system(s, SYS_THERMAL));
+    timer_end(s, PH_THERMAL_ASSEMBLE);
+    TRY(band_solve_refined(s, s->thermal, s->opt.thermal_rtol, s->opt.max_iters, st));
+    TRY(thermal_post(s, s->thermal.x));
+    TRY(read_scalars(s));
+    s->last_maxDT = slot(s, X_DT);
+    if (maxDT) *maxDT = s->last_maxDT;
+    return EREBUS_OK;
+}
+
+int erebus_nodes_to_markers(erebus_state *s, double dt, int32_t timestep) {
+    if (!s) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    TRY(nodes_to_markers(s, dt, timestep));
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "nodes_to_markers");
+}
+
+int erebus_advect_rk4(erebus_state *s, double dt) {
+    if (!s) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    TRY(velocities_rotation(s));
+    TRY(advect(s, dt));
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "advect");
+}
+
+int erebus_replenish(erebus_state *s, int32_t timestep, int64_t *marknum) {
+    if (!s) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    return replenish(s, timestep, marknum);
+}
+
+// One timestep (E:6370-7235).
+int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st) {
+    if (!s || timestep < 1) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    const ErebusParams &p = s->p;
+    ErebusStepStats stats = {};
+    double worst = 0.0;
+    int hydro_f0 = s->hydro.factorizations, th_f0 = s->thermal.factorizations;
+    timer_begin(s, PH_MARKERS_TO_NODES);
+    TRY(markers_to_nodes(s, s->timesum));
+    timer_end(s, PH_MARKERS_TO_NODES);
+    ErebusSolveStats gs = {};
+    timer_begin(s, PH_GRAVITY);
+    TRY(erebus_gravity(s, &gs));
+    timer_end(s, PH_GRAVITY);
+    stats.gravity_iters = gs.iterations;
+    worst = gs.rel_residual;
+    double dt = std::fmin(s->dt * p.dtcoefup, p.dt_longest);   // E:6619
+    size_t npb = (size_t)s->g.Nx1 * s->g.Ny1 * 8, nbb = (size_t)s->g.Nx * s->g.Ny;
+    for (int titer = 1; titer <= p.titermax; titer++) {
+        stats.titer = titer;
+        timer_begin(s, PH_REACTION);
+        if (p.reaction_active) TRY(thermochemical_reaction(s, dt, timestep, titer));
+        timer_end(s, PH_REACTION);
+        // E:6658-6669
+        cudaMemcpyAsync(s->grid[G_ETA00], s->grid[G_ETA], nbb * 8, cudaMemcpyDeviceToDevice,
+                        s->stream);
+        cudaMemcpyAsync(s->grid[G_YNY00], s->grid[G_YNY], nbb, cudaMemcpyDeviceToDevice,
+                        s->stream);
+        if (timestep == 1) cudaMemsetAsync(s->grid[G_BETAPHI], 0, npb, s->stream);
+        cudaMemcpyAsync(s->grid[G_pr0], s->grid[G_pr], npb, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(s->grid[G_pf0], s->grid[G_pf], npb, cudaMemcpyDeviceToDevice, s->stream);
+        for (int iplast = 1; iplast <= p.titermax; iplast++) {
+            stats.iplast_total++;
+            int conv = 0;
+            ErebusSolveStats hs = {};
+            TRY(erebus_hydromech_pass(s, &dt, iplast, &conv, &hs));
+            stats.krylov_total += hs.iterations;
+            worst = std::fmax(worst, hs.rel_residual);
+            if (conv) break;
+        }
+        ErebusSolveStats ts = {};
+        double maxDT = 0.0;
+        TRY(erebus_thermal_solve(s, dt, timestep, &maxDT, &ts));
+        stats.thermal_total += ts.iterations;
+        worst = std::fmax(worst, ts.rel_residual);
+        if (titer == 1 && maxDT > p.DTmax) dt *= p.DTmax * (1.0 / maxDT);   // E:4187-4197
+        double pferr = slot(s, X_PFERR), dmpmax = slot(s, X_DMP);        // E:4216-4223
+        if (pferr < p.pferrmax && (titer > 2 || dmpmax <= 0.0)) break;
+    }
+    timer_begin(s, PH_NODES_TO_MARKERS);
+    TRY(nodes_to_markers(s, dt, timestep));
+    TRY(velocities_rotation(s));
+    timer_end(s, PH_NODES_TO_MARKERS);
+    TRY(advect(s, dt));
+    int64_t n = 0;
+    timer_begin(s, PH_REPLENISH);
+    TRY(replenish(s, timestep, &n));
+    timer_end(s, PH_REPLENISH);
+    s->dt = dt;
+    s->timesum += dt;
+    stats.marknum = s->marknum;
+    stats.dt = dt;
+    stats.timesum = s->timesum;
+    stats.worst_rel_residual = worst;
+    stats.factorizations = (s->hydro.factorizations - hydro_f0) * 1000 + (s->thermal.factorizations - th_f0);
+    if (st) *st = stats;
+    return EREBUS_OK;
+}
+
+int erebus_export_hydromech(erebus_state *s, double dt, int64_t *nnz_out, int64_t *rows,
+                            int64_t *cols, double *vals, double *R) {
+    if (!s || !nnz_out) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    TRY(set_dev_dt(s, dt));
+    return export_system(s, SYS_HYDRO, nnz_out, rows, cols, vals, R);
+}
+
+int erebus_apply_hydromech(erebus_state *s, double dt, const double *x, double *y) {
+    if (!s || !x || !y) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    TRY(set_dev_dt(s, dt));
+    TRY(bulk_viscosity(s));
+    BandSystem &sys = s->hydro;
+    BandView B = band_view(sys);
+    // assemble into the ELL arrays without touching the factors
+    int64_t n = sys.n;
+    double *dx = nullptr, *dy = nullptr;
+    TRY(check_cuda(s, cudaMallocAsync(&dx, n * 8, s->stream), "apply alloc"));
+    TRY(check_cuda(s, cudaMallocAsync(&dy, n * 8, s->stream), "apply alloc"));
+    cudaMemcpyAsync(dx, x, n * 8, cudaMemcpyHostToDevice, s->stream);
+    TRY(assemble_system(s, SYS_HYDRO));
+    (void)B;
+    TRY(band_apply_unscaled(s, sys, dx, dy));
+    cudaMemcpyAsync(y, dy, n * 8, cudaMemcpyDeviceToHost, s->stream);
+    int rc = check_cuda(s, cudaStreamSynchronize(s->stream), "apply");
+    cudaFreeAsync(dx, s->stream);
+    cudaFreeAsync(dy, s->stream);
+    return rc;
+}
+
+}  // extern "C"

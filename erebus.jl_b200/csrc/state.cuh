@@ -1,0 +1,166 @@
+// state.cuh -- device-resident state of one planetesimal.
+#pragma once
+#include <string>
+#include <vector>
+#include "common.cuh"
+
+namespace erebus {
+
+// Marker fields, in the order of ErebusMarkersHost.  `tm` is stored as int8
+// on the device (values 1..3) and as int64 on the host.
+enum MarkerField {
+    M_xm, M_ym, M_tm, M_tkm, M_sxxm, M_sxym, M_etavpm, M_phim, M_phinewm,
+    M_pfm0, M_XWsolidm, M_XWsolidm0, M_rhototalm, M_rhocptotalm,
+    M_etatotalm, M_hrtotalm, M_ktotalm, M_tkm_rhocptotalm,
+    M_etafluidcur_inv_kphim, M_inv_gggtotalm, M_fricttotalm, M_cohestotalm,
+    M_tenstotalm, M_rhofluidcur, M_alphasolidcur, M_alphafluidcur,
+    M_etasolidm_m, M_COUNT
+};
+
+// Grid fields, in the order of ErebusGridHost.
+enum GridField {
+    G_ETA, G_ETA0, G_GGG, G_EXY, G_SXY, G_SXY0, G_wyx, G_COH, G_TEN, G_FRI,
+    G_YNY, G_ETA5, G_ETA00, G_YNY5, G_YNY00, G_YNY_inv_ETA, G_DSXY, G_DSY,
+    G_RHOX, G_RHOFX, G_KX, G_PHIX, G_vx, G_vxf, G_RX, G_qxD, G_gx,
+    G_RHOY, G_RHOFY, G_KY, G_PHIY, G_vy, G_vyf, G_RY, G_qyD, G_gy,
+    G_RHO, G_RHOCP, G_ALPHA, G_ALPHAF, G_HR, G_HA, G_HS, G_ETAP, G_GGGP,
+    G_EXX, G_SXX, G_SXX0, G_tk1, G_tk2, G_DT, G_DT0,
+    G_vxp, G_vyp, G_vxpf, G_vypf, G_pr, G_pf, G_ps, G_pr0, G_pf0, G_ps0,
+    G_ETAPHI, G_BETAPHI, G_PHI, G_APHI, G_FI, G_DMP, G_DHP, G_XWS,
+    G_EII, G_SII, G_DSXX, G_tk0, G_COUNT
+};
+constexpr int G_FIRST_P = G_RHOX;   // fields from here on are (Ny1,Nx1)
+
+// Scatter sums, in the order of ErebusSumsHost.
+enum SumField {
+    S_ETA0SUM, S_ETASUM, S_GGGSUM, S_SXYSUM, S_COHSUM, S_TENSUM, S_FRISUM,
+    S_WTSUM, S_RHOXSUM, S_RHOFXSUM, S_KXSUM, S_PHIXSUM, S_RXSUM, S_WTXSUM,
+    S_RHOYSUM, S_RHOFYSUM, S_KYSUM, S_PHIYSUM, S_RYSUM, S_WTYSUM, S_RHOSUM,
+    S_RHOCPSUM, S_ALPHASUM, S_ALPHAFSUM, S_HRSUM, S_GGGPSUM, S_SXXSUM,
+    S_TKSUM, S_PHISUM, S_DMPSUM, S_DHPSUM, S_XWSSUM, S_WTPSUM, S_COUNT
+};
+constexpr int S_FIRST_P = S_RHOXSUM;
+
+// Small device-side scalars read back by the host driver.
+struct DevScalars {
+    double dt;
+    double maxabs[8];          // reduction slots (bits of |x| as uint64)
+    double sum_ddd;            // plastic yielding error sum of squares
+    double norms[2];           // residual / right-hand side sums of squares
+    int    ynpl;
+    int    repl_count;         // markers to add in replenishment
+    int    err;                // device-side error flag
+    int    _pad;
+};
+enum MaxSlot { X_APHI = 0, X_VX, X_VY, X_VXF, X_VYF, X_DT, X_PFERR, X_DMP };
+
+// Cell-sorted marker index of one node set: the markers of cell c are
+// idx[start[c] .. start[c+1]) in ascending marker number.
+struct CellSort {
+    int ncells;
+    int *count, *start, *cursor, *idx, *tmp;
+};
+
+// Block-banded matrix (no pivoting LU) of one linear system.
+struct BandSystem {
+    int64_t n = 0;             // unknowns
+    int b = 0;                 // half bandwidth (max |row-col|)
+    int nb = 0;                // tile size
+    int NB = 0;                // tile rows/cols
+    int Bb = 0;                // tile half bandwidth
+    double *tiles = nullptr;   // NB * (2Bb+1) tiles of nb*nb, column-major
+    double *invL = nullptr;    // NB inverses of the unit-lower diagonal factors
+    double *invU = nullptr;    // NB inverses of the upper diagonal factors
+    double *rscale = nullptr;  // row scale (1/sum|row|)
+    double *rhs = nullptr;     // scaled right-hand side
+    double *x = nullptr;       // solution
+    double *r = nullptr;       // residual / correction work
+    double *d = nullptr;       // correction
+    double *ell_vals = nullptr;  // scaled entries per row (ELL, width `ell`)
+    int *ell_cols = nullptr;
+    int ell = 0;
+    double *ell_prev = nullptr;    // entries the current factors came from
+    int *changed = nullptr;        // set when the assembled matrix differs
+    unsigned int *bar = nullptr;   // grid barrier words
+    int *err = nullptr;            // device error flag of the LU kernels
+    bool factored = false;
+    int factorizations = 0;        // number of factorisations so far
+    int ph_factor = -1, ph_solve = -1;   // timer phases of this system
+};
+
+}  // namespace erebus
+
+struct erebus_state {
+    ErebusParams p;
+    ErebusSolverOptions opt;
+    erebus::Geo g;
+    int64_t capacity = 0;
+    int64_t marknum = 0;
+    double dt = 0.0, timesum = 0.0;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int64_t launches = 0;
+    std::string last_error;
+
+    // device memory
+    void *mem_markers = nullptr;
+    double *m[erebus::M_COUNT] = {};   // m[M_tm] is unused (tm8 holds tm)
+    int8_t *tm8 = nullptr;
+    double *grid[erebus::G_COUNT] = {};   // YNY* are uint8 stored in the slots
+    double *sums[erebus::S_COUNT] = {};
+    std::vector<void *> allocations;
+
+    erebus::CellSort sort[4];
+    double *r_dM = nullptr, *r_dH = nullptr;   // per-marker reaction outputs
+    int8_t *r_flag = nullptr;
+    double *tmp_node = nullptr;                // node-sized scratch
+    double *partials = nullptr;                // reduction partials
+    // replenishment scratch (per marker-grid anchor)
+    unsigned long long *a_mdis = nullptr;
+    int *a_mnum = nullptr, *a_src = nullptr, *a_rank = nullptr, *a_flag = nullptr;
+
+    erebus::DevScalars *dsc = nullptr;    // device scalars
+    erebus::DevScalars *hsc = nullptr;    // pinned host mirror
+
+    erebus::BandSystem hydro, thermal, gravity;
+    bool sorted_valid = false;
+    bool opt_no_reuse = false;   // refactorise every solve (testing)
+    double last_maxDT = 0.0;     // max|DT| of the last heat solve
+
+    // phase timing with CUDA events on `stream` (enabled on request)
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+    cudaEvent_t ev_open[32] = {};
+    double phase_ms[32] = {};
+    int64_t phase_count[32] = {};
+};
+
+namespace erebus {
+// Launch bookkeeping and error capture.
+int check_cuda(erebus_state *s, cudaError_t e, const char *what);
+#define EREBUS_LAUNCH(s, kernel, grid, block, smem, ...)                      \
+    do {                                                                      \
+        kernel<<<(grid), (block), (smem), (s)->stream>>>(__VA_ARGS__);        \
+        (s)->launches++;                                                      \
+    } while (0)
+
+// Phases timed by the event timer (erebus_phase_times).
+enum Phase {
+    PH_MARKERS_TO_NODES = 0, PH_GRAVITY, PH_REACTION, PH_HYDRO_ASSEMBLE,
+    PH_HYDRO_FACTOR, PH_HYDRO_SOLVE, PH_HYDRO_POST, PH_THERMAL_ASSEMBLE,
+    PH_THERMAL_FACTOR, PH_THERMAL_SOLVE, PH_NODES_TO_MARKERS, PH_RK4,
+    PH_BACKTRACE, PH_REPLENISH, PH_SCATTER_MERGE, PH_COUNT
+};
+void timer_begin(erebus_state *s, int phase);
+void timer_end(erebus_state *s, int phase);
+void timer_collect(erebus_state *s);   // after a stream sync
+
+// entry points of the kernel files (all enqueue on s->stream)
+int markers_to_nodes(erebus_state *s, double timesum);
+int thermochemical_reaction(erebus_state *s, double dt, int timestep, int titer);
+int nodes_to_markers(erebus_state *s, double dt, int timestep);
+int advect(erebus_state *s, double dt);
+int replenish(erebus_state *s, int timestep, int64_t *marknum);
+int build_cell_sort(erebus_state *s);
+}  // namespace erebus

@@ -160,8 +160,8 @@ typedef struct ErebusStepStats {
     int32_t iplast_total;      /* plastic iterations summed over titer */
     int32_t krylov_total;      /* Stokes-Darcy Krylov iterations summed */
     int32_t thermal_total;     /* heat-equation Krylov iterations summed */
-    int32_t gravity_iters;     /* gravity Krylov iterations */
-    int32_t _pad;
+    int32_t gravity_iters;     /* gravity refinement iterations */
+    int32_t factorizations;    /* LU factorisations (1000 * Stokes-Darcy + heat) */
     int64_t marknum;           /* markers in use after replenishment */
     double  dt;                /* timestep taken [s] */
     double  timesum;           /* model time after the step [s] */
@@ -252,11 +252,13 @@ int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st);
 
 /* ---- debugging / parity ----------------------------------------------- */
 /* Assembles the Stokes-Darcy system of E:3089-3572 from the current device
-   state and copies it out in CSC form (0-based, the reference's row order).
-   nnz_out receives the entry count; pass colptr/rowval/nzval = NULL to query
-   it.  R receives the right-hand side (6*Ny1*Nx1). */
+   state (with the given dt) and copies it out as COO triplets (0-based,
+   the reference's unknown order, entries of a row in the order of its
+   updateindex! calls).  nnz_out receives the entry count; pass
+   rows/cols/vals = NULL to query it.  R (may be NULL) receives the
+   right-hand side (6*Ny1*Nx1). */
 int erebus_export_hydromech(erebus_state *s, double dt, int64_t *nnz_out,
-                            int64_t *colptr, int64_t *rowval, double *nzval,
+                            int64_t *rows, int64_t *cols, double *vals,
                             double *R);
 /* Applies the device Stokes-Darcy operator y = L x (matrix-free, same
    coefficients as the assembled matrix). */
@@ -264,6 +266,18 @@ int erebus_apply_hydromech(erebus_state *s, double dt, const double *x,
                            double *y);
 /* Number of kernel launches issued by this state since creation. */
 int erebus_kernel_launches(const erebus_state *s, int64_t *count);
+/* The CUDA stream (cudaStream_t) all work of this state is enqueued on,
+   for callers that time it with their own events.  No reference
+   counterpart. */
+int erebus_get_stream(const erebus_state *s, void **stream);
+/* Per-phase device time measured with CUDA events on the state's stream
+   (no reference counterpart).  Phases, in order: markers->nodes, gravity,
+   reaction, Stokes-Darcy assembly, factorisation, triangular solves and
+   refinement, post-solve stencils, heat assembly, factorisation, solves,
+   nodes->markers, RK4 advection, pressure back-trace, replenishment,
+   scatter merge kernels.  Enabling resets the accumulators. */
+int erebus_enable_phase_timing(erebus_state *s, int32_t on);
+int erebus_phase_times(erebus_state *s, double *ms, int64_t *counts, int32_t n);
 
 #ifdef __cplusplus
 }
