@@ -654,6 +654,7 @@ int erebus_export_hydromech(erebus_state *s, double dt, int64_t *nnz_out, int64_
     if (!s || !nnz_out) return EREBUS_EINVAL;
     cudaSetDevice(s->device);
     TRY(set_dev_dt(s, dt));
+    TRY(bulk_viscosity(s));   // as the next plastic pass (E:6678)
     return export_system(s, SYS_HYDRO, nnz_out, rows, cols, vals, R);
 }
 

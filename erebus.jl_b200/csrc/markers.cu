@@ -50,10 +50,18 @@ __device__ __forceinline__ double ktotal(double ks, double kf, double phi) {
     return sqrt(ks * kf / 2 + (a * a) * (1.0 / 16.0)) -
            0.25 * (ks * (3.0 * phi - 2.0) + kf * (1.0 - 3.0 * phi));
 }
+// x^3 with one final rounding of a compensated product (Julia evaluates a
+// Float64 power with an integral exponent by compensated repeated
+// multiplication); x^2 is a single correctly rounded product.
+__device__ __forceinline__ double cube(double x) {
+    double hi = x * x, lo = fma(x, x, -hi);
+    double p = hi * x, e = fma(hi, x, -p);
+    return p + (e + lo * x);
+}
 __device__ __forceinline__ double etaf_inv_kphi(const ErebusParams &p, double k0,
                                                 double phi, double etaf) {
-    return etaf * (1.0 / k0) * pow(p.phim0 * (1.0 / phi), 3.0) *
-           pow((1.0 - phi) * (1.0 / (1.0 - p.phim0)), 2.0);
+    double r = (1.0 - phi) * (1.0 / (1.0 - p.phim0));
+    return etaf * (1.0 / k0) * cube(p.phim0 * (1.0 / phi)) * (r * r);
 }
 __device__ __forceinline__ double rhocpfluid(const ErebusParams &p, double T) {
     if (p.marker_property_mode == 1) {
@@ -439,7 +447,7 @@ int build_cell_sort(erebus_state *s) {
 template <int GRID, int MODE>
 static void launch_merge(erebus_state *s, MergeArgs a, int write_props) {
     GridSpec sp = grid_spec(s->g, GRID);
-    EREBUS_LAUNCH(s, (k_merge<GRID, MODE>), nblocks((int64_t)sp.rows * sp.cols), 128, 0,
+    EREBUS_LAUNCH(s, (k_merge<GRID, MODE>), nblocks((int64_t)sp.rows * sp.cols, 128), 128, 0,
                   s->g, mptr(s), a, gptr(s), write_props);
 }
 
@@ -803,7 +811,7 @@ int advect(erebus_state *s, double dt) {
     int n = (int)s->marknum;
     timer_begin(s, PH_RK4);
     if (n > 0)
-        EREBUS_LAUNCH(s, k_rk4, nblocks(n), 128, 0, s->p, s->g, mptr(s), gptr(s), n, dt);
+        EREBUS_LAUNCH(s, k_rk4, nblocks(n, 128), 128, 0, s->p, s->g, mptr(s), gptr(s), n, dt);
     timer_end(s, PH_RK4);
     timer_begin(s, PH_BACKTRACE);
     size_t np = (size_t)s->g.Nx1 * s->g.Ny1;

@@ -251,8 +251,10 @@ int erebus_replenish(erebus_state *s, int32_t timestep, int64_t *marknum);
 int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st);
 
 /* ---- debugging / parity ----------------------------------------------- */
-/* Assembles the Stokes-Darcy system of E:3089-3572 from the current device
-   state (with the given dt) and copies it out as COO triplets (0-based,
+/* Runs recompute_bulk_viscosity! (E:3634), then assembles the Stokes-Darcy
+   system of E:3089-3572 from the current device state (with the given dt),
+   i.e. the system the next plastic pass solves, and copies it out as COO
+   triplets (0-based,
    the reference's unknown order, entries of a row in the order of its
    updateindex! calls).  nnz_out receives the entry count; pass
    rows/cols/vals = NULL to query it.  R (may be NULL) receives the

@@ -182,11 +182,19 @@ static inline double ktotal(double ks, double kf, double phi) { /* E:1226 */
     return sqrt(ks * kf / 2 + (a * a) * (1.0 / 16.0)) -
            0.25 * (ks * (3.0 * phi - 2.0) + kf * (1.0 - 3.0 * phi));
 }
+/* x^3.0 and x^2.0 of E:1274: Julia evaluates a Float64 power with an
+   integral exponent by compensated repeated multiplication (one final
+   rounding); x^2 is a single correctly rounded product. */
+static inline double cube(double x) {
+    double hi = x * x, lo = fma(x, x, -hi);
+    double p = hi * x, e = fma(hi, x, -p);
+    return p + (e + lo * x);
+}
 /* eta_f / k(phi), Kozeny-Carman (E:1273-1275) */
 static inline double etaf_inv_kphi(const ErebusParams *p, double k0,
                                    double phi, double etaf) {
-    return etaf * (1.0 / k0) * pow(p->phim0 * (1.0 / phi), 3.0) *
-           pow((1.0 - phi) * (1.0 / (1.0 - p->phim0)), 2.0);
+    double r = (1.0 - phi) * (1.0 / (1.0 - p->phim0));
+    return etaf * (1.0 / k0) * cube(p->phim0 * (1.0 / phi)) * (r * r);
 }
 static inline double Q_radiogenic(double f, double ratio, double E,
                                   double tau, double time) { /* E:1294 */
