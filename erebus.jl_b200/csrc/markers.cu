@@ -986,3 +986,164 @@ int replenish(erebus_state *s, int timestep, int64_t *marknum) {
 }
 
 }  // namespace erebus
+
+// ---------------------------------------------------------------------------
+// Allocation-free marker -> node pass (erebus_markers_to_nodes_noalloc)
+//
+// For callers that own all device memory themselves (a host framework with
+// its own pool allocator, an application held to a fixed device-memory
+// budget): the pass takes the caller's device buffers for inputs and
+// outputs and keeps its scratch -- the four cell sorts and the weighted
+// sums of one node set -- in the file-scope array below, so no call
+// allocates.  The array occupies about 6.4 MB on every GPU that loads the
+// library, until the process exits.  All calls share it and it keeps the
+// last call's contents (counters are cleared at the start of each call);
+// calls that overlap on the GPU race.
+// ---------------------------------------------------------------------------
+namespace erebus {
+
+constexpr size_t NA_MARKERS = EREBUS_NOALLOC_MAX_MARKERS;
+constexpr size_t NA_NODES = EREBUS_NOALLOC_MAX_NODES;
+constexpr size_t NA_SUM_BYTES = 10 * NA_NODES * sizeof(double);
+constexpr size_t NA_SORT_INTS = 4 * (3 * (NA_NODES + 1) + 2 * NA_MARKERS);
+constexpr size_t NA_BYTES =
+    ((NA_SUM_BYTES + NA_SORT_INTS * sizeof(int) + NA_MARKERS + 256 + 255) / 256) * 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+// tm (int64, the caller's layout) -> int8; types outside 1..3 become 3 (so
+// every table index stays in range) and raise *err.
+__global__ void k_noalloc_tm(const int64_t *tm, int8_t *tm8, int n, int *err) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    int64_t t = tm[m];
+    if (t < 1 || t > 3) {
+        atomicExch(err, 1);
+        t = 3;
+    }
+    tm8[m] = (int8_t)t;
+}
+
+}  // namespace erebus
+
+#include <mutex>
+
+extern "C" int erebus_markers_to_nodes_noalloc(const ErebusParams *p,
+                                               const ErebusMarkersDevice *md,
+                                               int64_t marknum,
+                                               const ErebusGridDevice *gd,
+                                               double timesum, void *stream_) {
+    using namespace erebus;
+    if (!p || !md || !gd || marknum < 0) return EREBUS_EINVAL;
+    if (erebus_check_params(p) != EREBUS_OK) return EREBUS_EINVAL;
+    Geo g = make_geo(*p);
+    if (marknum > (int64_t)NA_MARKERS || (size_t)g.Nx1 * g.Ny1 > NA_NODES)
+        return EREBUS_ECAPACITY;
+    const void *const *mp = reinterpret_cast<const void *const *>(md);
+    for (int f = 0; f < M_COUNT; f++)
+        if (!mp[f] && !(f == M_etasolidm_m && !p->per_marker_eta)) return EREBUS_EINVAL;
+    const void *need[] = {gd->ETA0, gd->ETA, gd->GGG, gd->SXY0, gd->COH, gd->TEN, gd->FRI,
+                          gd->YNY, gd->RHOX, gd->RHOFX, gd->KX, gd->PHIX, gd->RX, gd->RHOY,
+                          gd->RHOFY, gd->KY, gd->PHIY, gd->RY, gd->RHO, gd->RHOCP, gd->ALPHA,
+                          gd->ALPHAF, gd->HR, gd->GGGP, gd->SXX0, gd->tk1, gd->PHI,
+                          gd->BETAPHI};
+    for (const void *q : need)
+        if (!q) return EREBUS_EINVAL;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream_);
+
+    // Set-up, once per device with that device current: the device address
+    // of the scratch array (its host-side name is only a stand-in).
+    static std::mutex mu;
+    static unsigned char *scratch_of[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EREBUS_ECUDA;
+    unsigned char *base;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!scratch_of[dev]) {
+            void *ptr = nullptr;
+            if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
+                return EREBUS_ECUDA;
+            scratch_of[dev] = static_cast<unsigned char *>(ptr);
+        }
+        base = scratch_of[dev];
+    }
+
+    // carve the scratch
+    double *sums = reinterpret_cast<double *>(base);
+    int *ip = reinterpret_cast<int *>(base + NA_SUM_BYTES);
+    SortPtrs S;
+    for (int gr = 0; gr < 4; gr++) {
+        GridSpec sp = grid_spec(g, gr);
+        S.ncells[gr] = sp.rows * sp.cols;
+        S.count[gr] = ip;  ip += NA_NODES + 1;
+        S.cursor[gr] = ip; ip += NA_NODES + 1;
+        S.start[gr] = ip;  ip += NA_NODES + 1;
+        S.idx[gr] = ip;    ip += NA_MARKERS;
+        S.tmp[gr] = ip;    ip += NA_MARKERS;
+    }
+    int8_t *tm8 = reinterpret_cast<int8_t *>(ip);
+    int *err = reinterpret_cast<int *>(base + NA_BYTES - 256);
+
+    MP M;
+    for (int f = 0; f < M_COUNT; f++) M.f[f] = const_cast<double *>(static_cast<const double *>(mp[f]));
+    M.f[M_tm] = nullptr;
+    M.tm = tm8;
+    GPtr G;
+    const void *const *gp = reinterpret_cast<const void *const *>(gd);
+    for (int f = 0; f < G_COUNT; f++) G.f[f] = const_cast<double *>(static_cast<const double *>(gp[f]));
+
+    // calculate_radioactive_heating (E:1336-1357), on the host
+    Heat h = {};
+    if (p->hr_al) {
+        double Q = p->f_al * p->ratio_al * p->E_al * exp(-timesum * (1.0 / g.tau_al)) *
+                   (1.0 / g.tau_al);
+        h.hrs[0] = Q * p->rhosolidm[0];
+        h.hrs[1] = Q * p->rhosolidm[1];
+    }
+    if (p->hr_fe) {
+        double Q = p->f_fe * p->ratio_fe * p->E_fe * exp(-timesum * (1.0 / g.tau_fe)) *
+                   (1.0 / g.tau_fe);
+        h.hrf[0] = Q * p->rhofluidm[0];
+    }
+
+    int n = (int)marknum;
+    cudaMemsetAsync(err, 0, sizeof(int), st);
+    for (int gr = 0; gr < 4; gr++) {
+        cudaMemsetAsync(S.count[gr], 0, sizeof(int) * S.ncells[gr], st);
+        cudaMemsetAsync(S.cursor[gr], 0, sizeof(int) * S.ncells[gr], st);
+    }
+    if (n > 0) {
+        k_noalloc_tm<<<nblocks(n), kThreads, 0, st>>>(
+            reinterpret_cast<const int64_t *>(mp[M_tm]), tm8, n, err);
+        k_marker_props<<<nblocks(n), kThreads, 0, st>>>(*p, g, M, n, h);
+        k_sort_count<<<nblocks(n), kThreads, 0, st>>>(g, M.f[M_xm], M.f[M_ym], n, S);
+    }
+    k_sort_scan<<<4, 1024, 0, st>>>(S);
+    if (n > 0) k_sort_place<<<nblocks(n), kThreads, 0, st>>>(g, M.f[M_xm], M.f[M_ym], n, S);
+    for (int gr = 0; gr < 4; gr++)
+        k_sort_segments<<<nblocks((int64_t)S.ncells[gr] * 32), kThreads, 0, st>>>(S, gr);
+    auto args = [&](int gr) {
+        MergeArgs a = {};
+        a.start = S.start[gr];
+        a.idx = S.idx[gr];
+        for (int f = 0; f < 10; f++) a.sums[f] = sums + (size_t)f * NA_NODES;
+        return a;
+    };
+    auto blocks = [&](int gr) {
+        GridSpec sp = grid_spec(g, gr);
+        return nblocks((int64_t)sp.rows * sp.cols, 128);
+    };
+    k_merge<GB, MM_SCATTER><<<blocks(GB), 128, 0, st>>>(g, M, args(GB), G, 1);
+    k_merge<GVX, MM_SCATTER><<<blocks(GVX), 128, 0, st>>>(g, M, args(GVX), G, 1);
+    k_merge<GVY, MM_SCATTER><<<blocks(GVY), 128, 0, st>>>(g, M, args(GVY), G, 1);
+    k_merge<GP, MM_SCATTER><<<blocks(GP), 128, 0, st>>>(g, M, args(GP), G, 1);
+    k_insulate_rows<<<nblocks(g.Nx1), kThreads, 0, st>>>(g, G.f[G_tk1]);
+    k_insulate_cols<<<nblocks(g.Ny1), kThreads, 0, st>>>(g, G.f[G_tk1]);
+    int herr = 0;
+    if (cudaGetLastError() != cudaSuccess) return EREBUS_ECUDA;
+    if (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return EREBUS_ECUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return EREBUS_ECUDA;
+    return herr ? EREBUS_EINVAL : EREBUS_OK;
+}

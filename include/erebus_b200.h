@@ -281,6 +281,44 @@ int erebus_get_stream(const erebus_state *s, void **stream);
 int erebus_enable_phase_timing(erebus_state *s, int32_t on);
 int erebus_phase_times(erebus_state *s, double *ms, int64_t *counts, int32_t n);
 
+/* ---- allocation-free marker -> node pass ------------------------------- */
+/* Device-pointer views: the same layouts as the host structs above, with
+   every pointer a device address (tm is int64 on the device too). */
+typedef ErebusMarkersHost ErebusMarkersDevice;
+typedef ErebusGridHost ErebusGridDevice;
+
+/* Largest problem the allocation-free pass accepts. */
+#define EREBUS_NOALLOC_MAX_MARKERS 131072
+#define EREBUS_NOALLOC_MAX_NODES 16384   /* (Ny+1)*(Nx+1), e.g. up to 127x127 */
+
+/* No counterpart in the reference (an addition of this library).
+   Same computation as erebus_markers_to_nodes, for callers that cannot let
+   a library allocate device memory: a host framework that owns every
+   device buffer through its own pool (a Julia GPU-array pool, for
+   instance) or an application held to a fixed device-memory budget.  For
+   them a hidden cudaMalloc would escape their accounting, can fail once
+   their pool holds the device, and synchronises the whole device.
+   The caller passes device pointers for all inputs and outputs: m (the
+   marker SoA; the seven derived marker properties are written back into
+   it) and g (the node fields of compute_{basic,vx,vy,p}_node_properties!
+   and tk1; other pointers of g may be NULL).  Scratch (the cell sort and
+   the weighted sums) is a file-scope device array of about 6.4 MB that
+   every GPU which loads the library keeps until the process exits.  The
+   call allocates nothing.  Its first call on a device looks up that
+   array's device address and should come before any stream capture.
+   marknum above EREBUS_NOALLOC_MAX_MARKERS or a grid with more than
+   EREBUS_NOALLOC_MAX_NODES nodes returns EREBUS_ECAPACITY without
+   launching anything; a marker type outside 1..3 returns EREBUS_EINVAL.
+   All calls share the scratch array: calls that overlap on the GPU (two
+   streams, two host threads) race and give wrong results.  `stream` is a
+   cudaStream_t (NULL = legacy default stream); the call returns after the
+   stream has drained. */
+int erebus_markers_to_nodes_noalloc(const ErebusParams *p,
+                                    const ErebusMarkersDevice *m,
+                                    int64_t marknum,
+                                    const ErebusGridDevice *g,
+                                    double timesum, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
