@@ -59,208 +59,513 @@ __device__ void grid_barrier(unsigned int *bar, int *err) {
 }
 
 // ---------------------------------------------------------------------------
-// tile kernels (one CTA, 256 threads, nb = 64)
+// tile primitives (one CTA of 256 threads, 64 x 64 FP64 tiles)
+//
+// Register layout of a tile held by the CTA: thread (ty, tx) = (tid/16,
+// tid%16) owns rows r = ty + 16 i and columns c = tx + 16 j, i, j = 0..3.
+// Shared-memory tiles are column-major with leading dimension LDS = 65
+// (conflict-free staging).  Data another CTA wrote during this kernel is
+// read with ld.global.cg (L2), never through the non-coherent L1.
 // ---------------------------------------------------------------------------
-// mode 0: C -= A * B; mode 1: C = A * B (C may alias A or B).
-// Shared memory: As[k][r] and Bt[k][c], 2 * 64 * 64 doubles.
-__device__ void tile_gemm(const double *A, const double *Bm, double *C, int mode,
-                          double *smem) {
-    constexpr int nb = NB_TILE;
-    double *As = smem, *Bt = smem + nb * nb;
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-        As[e] = A[e];                          // As[k*nb + r] = A(r,k)
-        int k = e % nb, c = e / nb;            // B(k,c) at e
-        Bt[k * nb + c] = Bm[e];
+constexpr int LDS = NB_TILE + 1;
+constexpr int STILE = NB_TILE * LDS;            // doubles per staged tile
+
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// global column-major tile -> smem column-major (ld LDS)
+__device__ __forceinline__ void stage_tile(double *dst, const double *src) {
+    const double2 *s2 = reinterpret_cast<const double2 *>(src);
+    double2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = __ldcg(&s2[threadIdx.x + 256 * q]);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        int e = 2 * (threadIdx.x + 256 * q), r = e % NB_TILE, c = e / NB_TILE;
+        dst[c * LDS + r] = v[q].x;
+        dst[c * LDS + r + 1] = v[q].y;
     }
-    __syncthreads();
+}
+// global column-major tile -> smem transposed (Bt[k*LDS + c] = B(k, c))
+__device__ __forceinline__ void stage_tile_t(double *dst, const double *src) {
+    const double2 *s2 = reinterpret_cast<const double2 *>(src);
+    double2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = __ldcg(&s2[threadIdx.x + 256 * q]);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        int e = 2 * (threadIdx.x + 256 * q), k = e % NB_TILE, c = e / NB_TILE;
+        dst[k * LDS + c] = v[q].x;
+        dst[(k + 1) * LDS + c] = v[q].y;
+    }
+}
+// smem column-major (ld LDS) -> global column-major
+__device__ __forceinline__ void unstage_tile(double *dst, const double *src) {
+    double2 *d2 = reinterpret_cast<double2 *>(dst);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        int e = 2 * (threadIdx.x + 256 * q), r = e % NB_TILE, c = e / NB_TILE;
+        d2[threadIdx.x + 256 * q] = make_double2(src[c * LDS + r], src[c * LDS + r + 1]);
+    }
+}
+__device__ __forceinline__ void regs_from_smem(const double *S, double a[4][4]) {
     int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double acc[4][4];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-#pragma unroll 8
-    for (int k = 0; k < nb; k++) {
-        double2 a01 = *reinterpret_cast<const double2 *>(&As[k * nb + ty * 4]);
-        double2 a23 = *reinterpret_cast<const double2 *>(&As[k * nb + ty * 4 + 2]);
-        double2 b01 = *reinterpret_cast<const double2 *>(&Bt[k * nb + tx * 4]);
-        double2 b23 = *reinterpret_cast<const double2 *>(&Bt[k * nb + tx * 4 + 2]);
-        double av[4] = {a01.x, a01.y, a23.x, a23.y};
-        double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+        for (int j = 0; j < 4; j++) a[i][j] = S[(tx + 16 * j) * LDS + ty + 16 * i];
+}
+__device__ __forceinline__ void regs_to_smem(double *S, const double a[4][4]) {
+    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
 #pragma unroll
-        for (int a = 0; a < 4; a++)
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int b = 0; b < 4; b++) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        for (int j = 0; j < 4; j++) S[(tx + 16 * j) * LDS + ty + 16 * i] = a[i][j];
+}
+// acc (+)= A * B with As column-major (ld LDS) and Bt transposed (ld LDS)
+__device__ __forceinline__ void gemm_acc(const double *As, const double *Bt, double acc[4][4]) {
+    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+#pragma unroll 4
+    for (int k = 0; k < NB_TILE; k++) {
+        double av[4], bv[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) av[i] = As[k * LDS + ty + 16 * i];
+#pragma unroll
+        for (int j = 0; j < 4; j++) bv[j] = Bt[k * LDS + tx + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
     }
-    __syncthreads();
-#pragma unroll
-    for (int b = 0; b < 4; b++)
-#pragma unroll
-        for (int a = 0; a < 4; a++) {
-            int r = ty * 4 + a, c = tx * 4 + b;
-            double *p = &C[c * nb + r];
-            *p = mode == 0 ? *p - acc[a][b] : acc[a][b];
-        }
 }
 
-// LU (no pivoting) of the tile at T in place, and the inverses of its unit
-// lower factor (Li) and upper factor (Ui).  Shared memory: 3 * nb * nb.
-__device__ void tile_lu_inv(double *T, double *Li, double *Ui, double *smem, int *err) {
-    constexpr int nb = NB_TILE;
-    double *A = smem, *X = smem + nb * nb, *Y = smem + 2 * nb * nb;
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) A[e] = T[e];
-    __syncthreads();
-    for (int k = 0; k < nb; k++) {
-        double piv = A[k * nb + k];
-        if (threadIdx.x == 0 && !(piv != 0.0)) atomicExch(err, 2);
-        for (int r = k + 1 + threadIdx.x; r < nb; r += blockDim.x) A[k * nb + r] /= piv;
-        __syncthreads();
-        int m = nb - k - 1;
-        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-            int r = k + 1 + e % m, c = k + 1 + e / m;
-            A[c * nb + r] -= A[k * nb + r] * A[c * nb + k];
-        }
-        __syncthreads();
-    }
-    // inverses: one thread per column
-    int c = threadIdx.x;
-    if (c < nb) {
-        // X = U^{-1}: U X = I, back substitution in column c
-        for (int r = nb - 1; r >= 0; r--) {
-            double s = (r == c) ? 1.0 : 0.0;
-            for (int k = r + 1; k < nb; k++) s -= A[k * nb + r] * X[c * nb + k];
-            X[c * nb + r] = r > c ? 0.0 : s / A[r * nb + r];
-        }
-    } else if (c < 2 * nb) {
-        c -= nb;
-        // Y = L^{-1} (unit lower): forward substitution in column c
-        for (int r = 0; r < nb; r++) {
-            double s = (r == c) ? 1.0 : 0.0;
-            for (int k = 0; k < r; k++) s -= A[k * nb + r] * Y[c * nb + k];
-            Y[c * nb + r] = r < c ? 0.0 : s;
-        }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-        T[e] = A[e];
-        Ui[e] = X[e];
-        Li[e] = Y[e];
-    }
-    __syncthreads();
-}
-
-__global__ void __launch_bounds__(LU_THREADS)
-k_band_factor(BandView B, unsigned int *bar, int *err) {
-    extern __shared__ double smem[];
-    constexpr int nb = NB_TILE;
-    const int NB = B.NB, Bb = B.Bb;
-    const int64_t t2 = (int64_t)nb * nb;
-    for (int K = 0; K < NB; K++) {
-        if (blockIdx.x == 0)
-            tile_lu_inv(tile_ptr(B, K, K), B.invL + K * t2, B.invU + K * t2, smem, err);
-        grid_barrier(bar, err);
-        int nJ = min(Bb, NB - 1 - K);
-        for (int t = blockIdx.x; t < 2 * nJ; t += gridDim.x) {
-            if (t < nJ) {   // U tile: A_KJ <- L_KK^{-1} A_KJ
-                double *T = tile_ptr(B, K, K + 1 + t);
-                tile_gemm(B.invL + K * t2, T, T, 1, smem);
-            } else {        // L tile: A_IK <- A_IK U_KK^{-1}
-                double *T = tile_ptr(B, K + 1 + (t - nJ), K);
-                tile_gemm(T, B.invU + K * t2, T, 1, smem);
+// In-place Gauss-Jordan inverse (no pivoting) of the tile held in registers
+// `a` (the layout above): step k publishes column k and row k, then every
+// thread updates its 16 elements branch-free; one barrier per step
+// (broadcast vectors double-buffered).  A zero or non-finite pivot raises
+// *err = 2.
+__device__ void tile_inverse(double a[4][4], double *vec, int *err) {
+    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+#pragma unroll
+    for (int kq = 0; kq < 4; kq++)
+        for (int kk = 0; kk < 16; kk++) {
+            const int k = kq * 16 + kk;
+            double *col = vec + (k & 1) * 2 * NB_TILE, *row = col + NB_TILE;
+            if (tx == kk) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) col[ty + 16 * i] = a[i][kq];
+            }
+            if (ty == kk) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) row[tx + 16 * j] = a[kq][j];
             }
             __syncthreads();
+            double piv = row[k];
+            if (threadIdx.x == 0 && !(fabs(piv) > 0.0 && fabs(piv) < INFINITY)) atomicExch(err, 2);
+            double ip = 1.0 / piv;
+            double f[4], rk[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) f[i] = col[ty + 16 * i] * ip;
+#pragma unroll
+            for (int j = 0; j < 4; j++) rk[j] = row[tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) a[i][j] = fma(-f[i], rk[j], a[i][j]);
+            // column k (rows != k), then row k, then the pivot
+            if (tx == kk) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) a[i][kq] = -f[i];
+            }
+            if (ty == kk) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) a[kq][j] = rk[j] * ip;
+                if (tx == kk) a[kq][kq] = ip;
+            }
         }
-        grid_barrier(bar, err);
-        for (int t = blockIdx.x; t < nJ * nJ; t += gridDim.x) {
-            int a = t % nJ, b = t / nJ;
-            int I = K + 1 + a, J = K + 1 + b;
-            tile_gemm(tile_ptr(B, I, K), tile_ptr(B, K, J), tile_ptr(B, I, J), 0, smem);
-            __syncthreads();
-        }
-        grid_barrier(bar, err);
-    }
+    __syncthreads();
 }
 
-// y (+)= T * x for one nb x nb tile; 4 threads per row.  mode 0: y -= Tx,
-// mode 1: y = Tx.  x must not alias y.
-__device__ __forceinline__ void tile_gemv(const double *T, const double *x, double *y,
-                                          int mode) {
-    constexpr int nb = NB_TILE;
-    int r = threadIdx.x >> 2, q = threadIdx.x & 3;
-    double s = 0.0;
-#pragma unroll 4
-    for (int c = q * 16; c < q * 16 + 16; c++) s = fma(T[c * nb + r], x[c], s);
-    s += __shfl_xor_sync(0xffffffffu, s, 1);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    if (q == 0) y[r] = mode == 0 ? y[r] - s : s;
+struct FactorSmem {
+    double As[STILE], Bt[STILE], Cs[STILE];
+    double vec[2 * 2 * NB_TILE];
+};
+
+// Invert diagonal tile (K,K), whose updated values are in registers `a`,
+// and store the inverse in its place.
+__device__ void invert_and_store(const BandView &B, int K, double a[4][4], FactorSmem &S,
+                                 int *err) {
+    tile_inverse(a, S.vec, err);
+    regs_to_smem(S.Cs, a);
+    __syncthreads();
+    unstage_tile(tile_ptr(B, K, K), S.Cs);
+    __syncthreads();
 }
 
-// Forward (L, unit) then backward (U) substitution of b -> x in place on
-// `w` (length NB*nb).  CTA a of step K updates block K+1+a; the CTA that
-// updates block K+1 also solves it, so one grid barrier per step suffices.
-__global__ void __launch_bounds__(LU_THREADS)
-k_band_solve(BandView B, double *w, unsigned int *bar, int *err) {
-    __shared__ double xs[NB_TILE], ys[NB_TILE];
-    constexpr int nb = NB_TILE;
+// Right-looking block LU without pivoting, with inverted diagonal blocks:
+// A = L U with L_KK = I, L_IK = A_IK D_K^{-1}, U_KJ = A_KJ (the Schur-updated
+// blocks) and D_K the Schur-updated diagonal block, whose inverse replaces
+// tile (K,K).  Step K:
+//   (B) L_IK <- A_IK D_K^{-1} (tile products);
+//   (C) A_IJ -= L_IK A_KJ over the trailing band; CTA 0 takes (K+1,K+1) and
+//       inverts it right away (look-ahead), so step K+1 starts with D^{-1}.
+// Two grid barriers per step.
+__global__ void __launch_bounds__(LU_THREADS, 2)
+k_band_factor(BandView B, unsigned int *bar, int *err) {
+    extern __shared__ __align__(16) double smem_raw[];
+    FactorSmem &S = *reinterpret_cast<FactorSmem *>(smem_raw);
     const int NB = B.NB, Bb = B.Bb;
-    const int64_t t2 = (int64_t)nb * nb;
-    // forward: w_K <- L_KK^{-1} (w_K - sum L_KJ w_J)
     if (blockIdx.x == 0) {
-        if (threadIdx.x < nb) xs[threadIdx.x] = w[threadIdx.x];
+        double a[4][4];
+        stage_tile(S.Cs, tile_ptr(B, 0, 0));
         __syncthreads();
-        tile_gemv(B.invL, xs, ys, 1);
+        regs_from_smem(S.Cs, a);
         __syncthreads();
-        if (threadIdx.x < nb) w[threadIdx.x] = ys[threadIdx.x];
+        invert_and_store(B, 0, a, S, err);
     }
     grid_barrier(bar, err);
     for (int K = 0; K < NB - 1; K++) {
+        int nJ = min(Bb, NB - 1 - K);
+        // (B) L_IK = A_IK * D_K^{-1}; CTA 0 is left free for the look-ahead
+        int nw = gridDim.x > 1 ? gridDim.x - 1 : 1, w = gridDim.x > 1 ? (int)blockIdx.x - 1 : 0;
+        for (int t = w; w >= 0 && t < nJ; t += nw) {
+            double acc[4][4] = {};
+            double *T = tile_ptr(B, K + 1 + t, K);
+            stage_tile(S.As, T);
+            stage_tile_t(S.Bt, tile_ptr(B, K, K));
+            __syncthreads();
+            gemm_acc(S.As, S.Bt, acc);
+            regs_to_smem(S.Cs, acc);
+            __syncthreads();
+            unstage_tile(T, S.Cs);
+            __syncthreads();
+        }
+        grid_barrier(bar, err);
+        // (C) trailing update; task 0 = tile (K+1, K+1) on CTA 0
+        for (int t = blockIdx.x; t < nJ * nJ; t += gridDim.x) {
+            int aI = t % nJ, bJ = t / nJ;
+            int I = K + 1 + aI, J = K + 1 + bJ;
+            double acc[4][4];
+            stage_tile(S.As, tile_ptr(B, I, K));
+            stage_tile_t(S.Bt, tile_ptr(B, K, J));
+            stage_tile(S.Cs, tile_ptr(B, I, J));
+            __syncthreads();
+            regs_from_smem(S.Cs, acc);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = -acc[i][j];
+            gemm_acc(S.As, S.Bt, acc);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = -acc[i][j];
+            __syncthreads();
+            if (t == 0) {
+                invert_and_store(B, K + 1, acc, S, err);
+            } else {
+                regs_to_smem(S.Cs, acc);
+                __syncthreads();
+                unstage_tile(tile_ptr(B, I, J), S.Cs);
+                __syncthreads();
+            }
+        }
+        grid_barrier(bar, err);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// triangular solves: one thread-block cluster of SOLVE_P CTAs
+//
+// Tile row I is owned by CTA I % SOLVE_P, which keeps the partial sums of
+// its rows of the current window in shared memory.  Forward sweep (L has
+// identity diagonal blocks), step K: subtract L_IK y_K from the CTA's own
+// rows I in (K, K+nI]; row K+1 is then final.  Backward sweep, step K:
+// subtract U_IK x_K from the own rows I in [K-nI, K), and the owner of row
+// K-1 applies D_{K-1}^{-1}.  The owner of the row that becomes final
+// updates it first and pushes it into every CTA's row queue (DSMEM stores,
+// then a remote mbarrier arrive with release semantics at cluster scope);
+// each CTA waits for the rows in push order (acquire at cluster scope), so
+// steps need no cluster-wide barrier.  The tiles (and the right-hand side of
+// the row entering the window) a CTA needs at the next step are fetched
+// with TMA bulk copies into the other buffer while the current step runs.
+// Every wait is bounded in time.  Pushes run at most SOLVE_P + 1 rows ahead
+// of the slowest CTA (each CTA owns every SOLVE_P-th row), below the queue
+// depth SOLVE_Q, so a queue slot is never overwritten before it is read.
+// ---------------------------------------------------------------------------
+constexpr int SOLVE_P = 8;
+constexpr int SOLVE_MAXT = 3;       // tiles per CTA and step (rows + inverse)
+constexpr int SOLVE_RING = 4;       // owned-row slots
+constexpr int SOLVE_Q = 16;         // pushed-row queue depth
+
+struct SolveSmem {
+    double tiles[2][SOLVE_MAXT][NB_TILE * NB_TILE];
+    double rhs[2][NB_TILE];          // entering row of each buffered step
+    double ring[SOLVE_RING][NB_TILE];
+    double queue[SOLVE_Q][NB_TILE];  // finished rows pushed by their owners
+    double wk[NB_TILE];
+    double part[4][NB_TILE];
+    unsigned long long mbar[2];      // TMA buffers
+    unsigned long long qbar[SOLVE_Q];  // queue slots
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *b) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned long long *b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                             unsigned long long *b) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned long long *b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(smem_u32(b)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_try_cluster(unsigned long long *b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(smem_u32(b)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Remote arrive on the mbarrier at the same shared-memory offset in CTA `rank`.
+__device__ __forceinline__ void mbar_arrive_remote(unsigned long long *b, uint32_t rank) {
+    asm volatile(
+        "{\n .reg .b32 ra;\n mapa.shared::cluster.u32 ra, %0, %1;\n"
+        " mbarrier.arrive.release.cluster.shared::cluster.b64 _, [ra];\n}\n"
+        ::"r"(smem_u32(b)), "r"(rank) : "memory");
+}
+__device__ void mbar_wait(unsigned long long *b, uint32_t parity, int *err, bool cluster) {
+    if (cluster ? mbar_try_cluster(b, parity) : mbar_try(b, parity)) return;
+    unsigned long long t0 = globaltimer();
+    while (!(cluster ? mbar_try_cluster(b, parity) : mbar_try(b, parity))) {
+        if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
+            atomicExch(err, 3);
+            return;
+        }
+    }
+}
+
+// What CTA `me` loads for step K of a sweep: the tiles of its rows of the
+// window (forward L_IK, I in (K, K+nI]; backward U_IK, I in [K-nI, K)), the
+// inverse D_{K-1}^{-1} if it owns row K-1 (backward), and the right-hand
+// side of the row entering the window at step K if it owns it.  The row
+// finished at this step (K+1 forward, K-1 backward) comes first.
+struct StepLoad {
+    int n;
+    const double *src[SOLVE_MAXT];
+    int row[SOLVE_MAXT];            // target row, -1 for the inverse
+    int enter;                      // entering row (owned), or -1
+};
+__device__ __forceinline__ StepLoad step_load(const BandView &B, int K, bool fwd, int me,
+                                              bool first) {
+    StepLoad s;
+    s.n = 0;
+    s.enter = -1;
+    const int NB = B.NB, Bb = B.Bb;
+    if (fwd) {
+        if (K >= NB - 1) return s;
         int nI = min(Bb, NB - 1 - K);
-        for (int a = blockIdx.x; a < nI; a += gridDim.x) {
-            int I = K + 1 + a;
-            if (threadIdx.x < nb) xs[threadIdx.x] = w[(int64_t)K * nb + threadIdx.x];
-            __syncthreads();
-            tile_gemv(tile_ptr(B, I, K), xs, w + (int64_t)I * nb, 0);
-            __syncthreads();
-            if (a == 0) {
-                if (threadIdx.x < nb) xs[threadIdx.x] = w[(int64_t)I * nb + threadIdx.x];
-                __syncthreads();
-                tile_gemv(B.invL + I * t2, xs, ys, 1);
-                __syncthreads();
-                if (threadIdx.x < nb) w[(int64_t)I * nb + threadIdx.x] = ys[threadIdx.x];
+        for (int I = K + 1; I <= K + nI; I++)
+            if (I % SOLVE_P == me && s.n < SOLVE_MAXT) {
+                s.src[s.n] = tile_ptr(B, I, K);
+                s.row[s.n++] = I;
             }
-            __syncthreads();
-        }
-        grid_barrier(bar, err);
-    }
-    // backward: w_K <- U_KK^{-1} (w_K - sum U_KJ w_J)
-    if (blockIdx.x == 0) {
-        int K = NB - 1;
-        if (threadIdx.x < nb) xs[threadIdx.x] = w[(int64_t)K * nb + threadIdx.x];
-        __syncthreads();
-        tile_gemv(B.invU + K * t2, xs, ys, 1);
-        __syncthreads();
-        if (threadIdx.x < nb) w[(int64_t)K * nb + threadIdx.x] = ys[threadIdx.x];
-    }
-    grid_barrier(bar, err);
-    for (int K = NB - 1; K > 0; K--) {
+        int er = K + Bb;
+        if (!first && er < NB && er % SOLVE_P == me) s.enter = er;
+    } else {
+        if (K <= 0) return s;
         int nI = min(Bb, K);
-        for (int a = blockIdx.x; a < nI; a += gridDim.x) {
-            int I = K - 1 - a;
-            if (threadIdx.x < nb) xs[threadIdx.x] = w[(int64_t)K * nb + threadIdx.x];
-            __syncthreads();
-            tile_gemv(tile_ptr(B, I, K), xs, w + (int64_t)I * nb, 0);
-            __syncthreads();
-            if (a == 0) {
-                if (threadIdx.x < nb) xs[threadIdx.x] = w[(int64_t)I * nb + threadIdx.x];
-                __syncthreads();
-                tile_gemv(B.invU + I * t2, xs, ys, 1);
-                __syncthreads();
-                if (threadIdx.x < nb) w[(int64_t)I * nb + threadIdx.x] = ys[threadIdx.x];
+        for (int I = K - 1; I >= K - nI; I--)
+            if (I % SOLVE_P == me && s.n < SOLVE_MAXT - 1) {
+                s.src[s.n] = tile_ptr(B, I, K);
+                s.row[s.n++] = I;
             }
+        if ((K - 1) % SOLVE_P == me) {
+            s.src[s.n] = tile_ptr(B, K - 1, K - 1);
+            s.row[s.n++] = -1;
+        }
+        int er = K - Bb;
+        if (!first && er >= 0 && er % SOLVE_P == me) s.enter = er;
+    }
+    return s;
+}
+
+__device__ __forceinline__ void issue_load(const double *w, SolveSmem &S, const StepLoad &sl,
+                                           int stage) {
+    if (threadIdx.x != 0) return;
+    uint32_t bytes = sl.n * NB_TILE * NB_TILE * sizeof(double) +
+                     (sl.enter >= 0 ? NB_TILE * sizeof(double) : 0);
+    if (bytes == 0) return;
+    mbar_expect(&S.mbar[stage], bytes);
+    for (int q = 0; q < sl.n; q++)
+        tma_bulk_g2s(S.tiles[stage][q], sl.src[q], NB_TILE * NB_TILE * sizeof(double),
+                     &S.mbar[stage]);
+    if (sl.enter >= 0)
+        tma_bulk_g2s(S.rhs[stage], w + (int64_t)sl.enter * NB_TILE, NB_TILE * sizeof(double),
+                     &S.mbar[stage]);
+}
+
+// y = T v (column-major tile in smem, unpadded) with all 256 threads: four
+// column quarters per row, four independent chains each, reduced through
+// `part`.  mode 0: y -= T v; mode 1: y = T v.
+__device__ __forceinline__ void smem_gemv(const double *T, const double *v, double *y,
+                                          double (*part)[NB_TILE], int mode) {
+    int r = threadIdx.x & 63, q = threadIdx.x >> 6;
+    const double *t = T + q * 16 * NB_TILE + r;
+    const double *vv = v + q * 16;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 16; c += 4) {
+        s0 = fma(t[(c + 0) * NB_TILE], vv[c + 0], s0);
+        s1 = fma(t[(c + 1) * NB_TILE], vv[c + 1], s1);
+        s2 = fma(t[(c + 2) * NB_TILE], vv[c + 2], s2);
+        s3 = fma(t[(c + 3) * NB_TILE], vv[c + 3], s3);
+    }
+    part[q][r] = (s0 + s1) + (s2 + s3);
+    __syncthreads();
+    if (threadIdx.x < NB_TILE) {
+        double s = (part[0][r] + part[1][r]) + (part[2][r] + part[3][r]);
+        y[r] = mode == 0 ? y[r] - s : s;
+    }
+    __syncthreads();
+}
+
+// Push the finished row `src` (smem, 64 values) as queue entry `seq` into
+// every CTA of the cluster, and write it to global memory.
+__device__ __forceinline__ void push_row(cooperative_groups::cluster_group &cluster,
+                                         SolveSmem &S, const double *src, int seq,
+                                         double *wrow) {
+    int slot = seq % SOLVE_Q;
+    if (threadIdx.x < NB_TILE) {
+        double v = src[threadIdx.x];
+        wrow[threadIdx.x] = v;
+#pragma unroll
+        for (int c = 0; c < SOLVE_P; c++) {
+            double *dst = cluster.map_shared_rank(&S.queue[slot][0], c);
+            dst[threadIdx.x] = v;
+        }
+        asm volatile("fence.acq_rel.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x < SOLVE_P) mbar_arrive_remote(&S.qbar[slot], threadIdx.x);
+}
+
+__global__ void __cluster_dims__(SOLVE_P, 1, 1) __launch_bounds__(LU_THREADS, 1)
+k_band_solve(BandView B, double *w, int *err) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(128) double smem_raw[];
+    SolveSmem &S = *reinterpret_cast<SolveSmem *>(smem_raw);
+    const int me = (int)cluster.block_rank();
+    const int NB = B.NB, Bb = B.Bb;
+    auto slot = [&](int I) { return (I / SOLVE_P) % SOLVE_RING; };
+    uint32_t uses[2] = {0u, 0u};
+    if (threadIdx.x == 0) {
+        mbar_init(&S.mbar[0]);
+        mbar_init(&S.mbar[1]);
+        for (int q = 0; q < SOLVE_Q; q++) mbar_init(&S.qbar[q]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    cluster.sync();   // every queue barrier exists before the first push
+    int step = 0;     // running step index over both sweeps (buffer = step & 1)
+    for (int sweep = 0; sweep < 2; sweep++) {
+        const bool fwd = sweep == 0;
+        const int K0 = fwd ? 0 : NB - 1;
+        const int seq0 = fwd ? 0 : NB;   // queue sequence of the sweep's first row
+        // rows of the first window: [0, Bb] forward, [NB-1-Bb, NB-1] backward
+        int lo = fwd ? 0 : max(0, NB - 1 - Bb), hi = fwd ? min(NB - 1, Bb) : NB - 1;
+        for (int I = lo; I <= hi; I++)
+            if (I % SOLVE_P == me && threadIdx.x < NB_TILE)
+                S.ring[slot(I)][threadIdx.x] = __ldcg(&w[(int64_t)I * NB_TILE + threadIdx.x]);
+        StepLoad cur = step_load(B, K0, fwd, me, true);
+        issue_load(w, S, cur, step & 1);
+        __syncthreads();
+        if (K0 % SOLVE_P == me) {     // first row: y_0 = w_0; x_{NB-1} = D^{-1} y_{NB-1}
+            double *y = S.ring[slot(K0)];
+            if (!fwd) {
+                const double *inv = tile_ptr(B, K0, K0);
+                if (threadIdx.x < NB_TILE) S.wk[threadIdx.x] = y[threadIdx.x];
+                __syncthreads();
+                int r = threadIdx.x & 63, q = threadIdx.x >> 6;
+                double s = 0.0;
+                for (int c = q * 16; c < q * 16 + 16; c++)
+                    s = fma(__ldcg(&inv[c * NB_TILE + r]), S.wk[c], s);
+                S.part[q][r] = s;
+                __syncthreads();
+                if (threadIdx.x < NB_TILE)
+                    y[r] = (S.part[0][r] + S.part[1][r]) + (S.part[2][r] + S.part[3][r]);
+                __syncthreads();
+            }
+            push_row(cluster, S, y, seq0, w + (int64_t)K0 * NB_TILE);
+        }
+        const int nsteps = NB - 1;
+        for (int it = 0; it < nsteps; it++, step++) {
+            const int K = fwd ? it : NB - 1 - it;
+            const int Kn = fwd ? K + 1 : K - 1;      // row finished at this step
+            const int stage = step & 1;
+            StepLoad nxt;
+            nxt.n = 0;
+            nxt.enter = -1;
+            if (it + 1 < nsteps) {                 // prefetch the next step
+                nxt = step_load(B, fwd ? K + 1 : K - 1, fwd, me, false);
+                issue_load(w, S, nxt, stage ^ 1);
+            }
+            // the finished row K, pushed by its owner
+            const int seq = seq0 + it, qs = seq % SOLVE_Q;
+            mbar_wait(&S.qbar[qs], (uint32_t)(seq / SOLVE_Q) & 1u, err, true);
+            if (cur.n > 0 || cur.enter >= 0) {
+                mbar_wait(&S.mbar[stage], uses[stage] & 1u, err, false);
+                uses[stage]++;
+            }
+            if (cur.enter >= 0 && threadIdx.x < NB_TILE)
+                S.ring[slot(cur.enter)][threadIdx.x] = S.rhs[stage][threadIdx.x];
+            __syncthreads();
+            const double *yk = S.queue[qs];
+            const bool owner = Kn % SOLVE_P == me;
+            if (owner) {   // the row finished at this step first, then push it
+                double *y = S.ring[slot(Kn)];
+                if (fwd) {
+                    smem_gemv(S.tiles[stage][0], yk, y, S.part, 0);
+                } else {
+                    for (int q = 0; q < cur.n; q++)
+                        if (cur.row[q] == Kn) smem_gemv(S.tiles[stage][q], yk, y, S.part, 0);
+                    if (threadIdx.x < NB_TILE) S.wk[threadIdx.x] = y[threadIdx.x];
+                    __syncthreads();
+                    smem_gemv(S.tiles[stage][cur.n - 1], S.wk, y, S.part, 1);
+                }
+                push_row(cluster, S, y, seq + 1, w + (int64_t)Kn * NB_TILE);
+            }
+            for (int q = 0; q < cur.n; q++)
+                if (cur.row[q] >= 0 && !(owner && cur.row[q] == Kn))
+                    smem_gemv(S.tiles[stage][q], yk, S.ring[slot(cur.row[q])], S.part, 0);
+            cur = nxt;
+            fence_proxy_async();
             __syncthreads();
         }
-        grid_barrier(bar, err);
+        // the backward sweep reads the forward result (also through TMA)
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        __threadfence();
+        cluster.sync();
     }
+    for (int s = 0; s < 2; s++)
+        if (uses[s] > 0) mbar_wait(&S.mbar[s], (uses[s] - 1) & 1u, err, false);
+    cluster.sync();
 }
 
 // r = rhs - A x (scaled rows, ELL)
@@ -422,10 +727,10 @@ static int lu_error(erebus_state *s, BandSystem &sys, const char *what) {
 }
 
 int band_factor(erebus_state *s, BandSystem &sys) {
-    size_t smem = 3 * NB_TILE * NB_TILE * sizeof(double);
+    size_t smem = sizeof(FactorSmem);
     cudaFuncSetAttribute(k_band_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    int want = sys.Bb * sys.Bb > 2 * sys.Bb ? sys.Bb * sys.Bb : 2 * sys.Bb;
+    int want = 1 + (sys.Bb * sys.Bb > 2 * sys.Bb ? sys.Bb * sys.Bb : 2 * sys.Bb);
     int blocks = coop_blocks(s, (const void *)k_band_factor, LU_THREADS, smem, want);
     if (blocks < 1) {
         s->last_error = "band_factor: kernel does not fit";
@@ -446,18 +751,18 @@ int band_factor(erebus_state *s, BandSystem &sys) {
     return EREBUS_OK;
 }
 
+// In-place solve L U w = w with the cluster kernel.
 static int band_solve_inplace(erebus_state *s, BandSystem &sys, double *w) {
-    int blocks = coop_blocks(s, (const void *)k_band_solve, LU_THREADS, 0, sys.Bb);
+    if (sys.Bb > 2 * SOLVE_P) {
+        s->last_error = "band_solve: band too wide for the cluster solve";
+        return EREBUS_EINVAL;
+    }
+    size_t smem = sizeof(SolveSmem);
+    cudaFuncSetAttribute(k_band_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     BandView B = band_view(sys);
-    unsigned int *bar = sys.bar;
-    int *err = sys.err;
-    void *args[] = {&B, &w, &bar, &err};
-    cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
-    int rc = check_cuda(s, cudaLaunchCooperativeKernel((const void *)k_band_solve, blocks,
-                                                       LU_THREADS, args, 0, s->stream),
-                        "band_solve launch");
+    k_band_solve<<<SOLVE_P, LU_THREADS, smem, s->stream>>>(B, w, sys.err);
     s->launches++;
-    return rc;
+    return check_cuda(s, cudaGetLastError(), "band_solve launch");
 }
 
 int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir,
@@ -472,11 +777,13 @@ int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir
     timer_begin(s, sys.ph_solve);
     int64_t np = (int64_t)sys.NB * sys.nb;
     BandView B = band_view(sys);
-    cudaMemcpyAsync(sys.x, sys.rhs, np * 8, cudaMemcpyDeviceToDevice, s->stream);
-    rc = band_solve_inplace(s, sys, sys.x);
-    if (rc) return rc;
+    // Iterative refinement x <- x + (LU)^{-1} (b - A x), started from the
+    // previous solution of this system when there is one (the matrix or the
+    // right-hand side changed little since), else from zero.
+    bool cold = !sys.have_x;
+    if (cold) cudaMemsetAsync(sys.x, 0, np * 8, s->stream);
     double rel = 0.0;
-    int it = 0;
+    int solves = 0;
     for (;;) {
         EREBUS_LAUNCH(s, k_band_residual, nblocks(np), kThreads, 0, B, sys.x, sys.r);
         EREBUS_LAUNCH(s, k_norms2, 1, 1024, 0, sys.r, sys.rhs, np, &s->dsc->norms[0]);
@@ -487,16 +794,24 @@ int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir
         if (rc) return rc;
         double rr = s->hsc->norms[0], bb = s->hsc->norms[1];
         rel = bb > 0.0 ? sqrt(rr / bb) : sqrt(rr);
-        if (!(rel > rtol) || it >= max_ir) break;
+        if (rel <= rtol) break;
+        if (!(rel < INFINITY)) {            // NaN/Inf: restart once from zero
+            if (cold) break;
+            cudaMemsetAsync(sys.x, 0, np * 8, s->stream);
+            cold = true;
+            continue;
+        }
+        if (solves > max_ir) break;
         cudaMemcpyAsync(sys.d, sys.r, np * 8, cudaMemcpyDeviceToDevice, s->stream);
         rc = band_solve_inplace(s, sys, sys.d);
         if (rc) return rc;
         EREBUS_LAUNCH(s, k_axpy, nblocks(np), kThreads, 0, sys.x, sys.d, np);
-        it++;
+        solves++;
     }
     timer_end(s, sys.ph_solve);
+    sys.have_x = rel <= rtol;
     if (st) {
-        st->iterations = it;
+        st->iterations = solves;
         st->converged = rel <= rtol;
         st->rel_residual = rel;
     }

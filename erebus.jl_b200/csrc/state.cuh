@@ -84,6 +84,7 @@ struct BandSystem {
     unsigned int *bar = nullptr;   // grid barrier words
     int *err = nullptr;            // device error flag of the LU kernels
     bool factored = false;
+    bool have_x = false;           // x holds a converged solution
     int factorizations = 0;        // number of factorisations so far
     int ph_factor = -1, ph_solve = -1;   // timer phases of this system
 };
