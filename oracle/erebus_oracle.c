@@ -454,6 +454,24 @@ int oracle_markers_to_nodes(const ErebusParams *p, ErebusMarkersHost *M,
     return 0;
 }
 
+/* compute_relative_enthalpy (E:2502-2504) */
+static inline double rel_enthalpy(const ErebusParams *p, double Xs, double XW) {
+    return -Xs * XW * p->dHWD / (p->MD + p->MH2O);
+}
+/* compute_gibbs_free_energy (E:2470-2482) */
+static inline double gibbs(const ErebusParams *p, const Geo *g, double T, double pf,
+                           double XD, double XW, double dt, double dtr) {
+    if (dt < dtr)
+        return (p->dHWD - T * p->dSWD + pf * g->dVWD + p->RG * T * log(XD / XW)) *
+               (1.0 - dt / dtr);
+    return 0.0;
+}
+/* compute_reaction_constant (E:2521-2524) */
+static inline double reaction_constant(const ErebusParams *p, const Geo *g, double T,
+                                       double pf, double dG) {
+    return exp(-(p->dHWD - T * p->dSWD + g->dVWD * pf - dG) / (p->RG * T));
+}
+
 /* ------------------------------------------------------------------------ */
 /* thermochemical reaction (E:2558-2694)                                    */
 /* ------------------------------------------------------------------------ */
@@ -487,19 +505,9 @@ int oracle_thermochemical_reaction(const ErebusParams *p, ErebusMarkersHost *M,
         double rhos0 = (p->MD + p->MH2O * XW0) / (g.VDs * XD0 + g.VWs * XW0);
         double rhof0 = tknm > p->tmfluidphase ? p->rhoH2Of : p->rhoH2Ofi;
         double dtr = dtreaction_of(p, tknm, phi);
-        /* compute_relative_enthalpy (E:2502) */
-        double Ht0 = -Xs0 * XW0 * p->dHWD / (p->MD + p->MH2O);
-        /* compute_gibbs_free_energy (E:2470-2482) */
-        double dGWD0;
-        if (dt < dtr)
-            dGWD0 = (p->dHWD - tknm * p->dSWD + pfnm * g.dVWD +
-                     p->RG * tknm * log(XD0 / XW0)) *
-                    (1.0 - dt / dtr);
-        else
-            dGWD0 = 0.0;
-        /* compute_reaction_constant (E:2521-2524) */
-        double KWD = exp(-(p->dHWD - tknm * p->dSWD + g.dVWD * pfnm - dGWD0) /
-                         (p->RG * tknm));
+        double Ht0 = rel_enthalpy(p, Xs0, XW0);
+        double dGWD0 = gibbs(p, &g, tknm, pfnm, XD0, XW0, dt, dtr);
+        double KWD = reaction_constant(p, &g, tknm, pfnm, dGWD0);
         double XW1 = 1.0 / (KWD + 1.0);
         double XD1 = 1.0 - XW1;
         double Xs1 = XDt / (1.0 - XDt * XW1);
@@ -508,7 +516,7 @@ int oracle_thermochemical_reaction(const ErebusParams *p, ErebusMarkersHost *M,
             double phi1 = Xf1 * VH2O / (Xf1 * VH2O + Xs1 * (XW1 * g.VWs + XD1 * g.VDs));
             double rhos1 = (p->MD + p->MH2O * XW1) / (g.VDs * XD1 + g.VWs * XW1);
             double rhof1 = tknm > p->tmfluidphase ? p->rhoH2Of : p->rhoH2Ofi;
-            double Ht1 = -Xs1 * XW1 * p->dHWD / (p->MD + p->MH2O);
+            double Ht1 = rel_enthalpy(p, Xs1, XW1);
             double dHt = Ht1 - Ht0;
             double RV = (rhos1 * (1.0 - phi1) + rhof1 * phi1) /
                         (rhos0 * (1.0 - phi) + rhof0 * phi);
@@ -1440,4 +1448,66 @@ int64_t oracle_replenish(const ErebusParams *p, ErebusMarkersHost *M,
             }
         }
     return n;
+}
+
+/* ------------------------------------------------------------------------ */
+/* hooks for the tests that re-express the reference's unit tests          */
+/* ------------------------------------------------------------------------ */
+void oracle_fix_grid(const ErebusParams *p, int grid, double x, double y, int *i, int *j) {
+    Geo g = geo(p);
+    double w[4];
+    grid_weights(&g, grid, x, y, i, j, w);
+}
+void oracle_weights_grid(const ErebusParams *p, int grid, double x, double y, int *i,
+                         int *j, double *w) {
+    Geo g = geo(p);
+    grid_weights(&g, grid, x, y, i, j, w);
+}
+double oracle_ktotal(double ks, double kf, double phi) { return ktotal(ks, kf, phi); }
+double oracle_total(double s, double f, double phi) { return total(s, f, phi); }
+double oracle_etaf_inv_kphi(const ErebusParams *p, double k0, double phi, double etaf) {
+    return etaf_inv_kphi(p, k0, phi, etaf);
+}
+double oracle_Q_radiogenic(double f, double ratio, double E, double tau, double t) {
+    return Q_radiogenic(f, ratio, E, tau, t);
+}
+void oracle_radioactive_heating(const ErebusParams *p, double timesum, double *hrs,
+                                double *hrf) {
+    Geo g = geo(p);
+    radioactive_heating(p, &g, timesum, hrs, hrf);
+}
+double oracle_dtreaction(const ErebusParams *p, double T, double phi) {
+    return dtreaction_of(p, T, phi);
+}
+double oracle_rhocpfluid(const ErebusParams *p, double T) { return rhocpfluid(p, T); }
+double oracle_ksolid(const ErebusParams *p, double T) { return ksolid(p, T); }
+double oracle_kfluid(const ErebusParams *p, double T) { return kfluid(p, T); }
+double oracle_gibbs(const ErebusParams *p, double T, double pf, double XD, double XW,
+                    double dt, double dtr) {
+    Geo g = geo(p);
+    return gibbs(p, &g, T, pf, XD, XW, dt, dtr);
+}
+double oracle_rel_enthalpy(const ErebusParams *p, double Xs, double XW) {
+    return rel_enthalpy(p, Xs, XW);
+}
+double oracle_reaction_constant(const ErebusParams *p, double T, double pf, double dG) {
+    Geo g = geo(p);
+    return reaction_constant(p, &g, T, pf, dG);
+}
+/* marker_to_{basic,vx,vy,p}_nodes! over given marker properties (no
+   compute_marker_properties!), as the reference's scatter tests call them */
+void oracle_scatter_only(const ErebusParams *p, const ErebusMarkersHost *M, int64_t n,
+                         ErebusSumsHost *s) {
+    Geo g = geo(p);
+    reset_sums(&g, s);
+    for (int64_t m = 0; m < n; m++) scatter_marker(&g, M, m, s);
+}
+void oracle_node_properties(const ErebusParams *p, const ErebusSumsHost *s,
+                            ErebusGridHost *G) {
+    Geo g = geo(p);
+    node_properties(&g, s, G);
+}
+void oracle_insulating_bc(const ErebusParams *p, double *t) {
+    Geo g = geo(p);
+    insulating_bc(&g, t);
 }

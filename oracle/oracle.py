@@ -86,6 +86,24 @@ def lib():
             "oracle_backtrace_pressures": (I, [P, P, D]),
             "oracle_replenish": (I64, [P, P, I64, I64, P, P, I]),
             "oracle_u01": (D, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+            # pointwise hooks for the re-expressed reference unit tests
+            "oracle_fix_grid": (None, [P, I, D, D, P, P]),
+            "oracle_weights_grid": (None, [P, I, D, D, P, P, P]),
+            "oracle_ktotal": (D, [D, D, D]),
+            "oracle_total": (D, [D, D, D]),
+            "oracle_etaf_inv_kphi": (D, [P, D, D, D]),
+            "oracle_Q_radiogenic": (D, [D, D, D, D, D]),
+            "oracle_radioactive_heating": (None, [P, D, P, P]),
+            "oracle_dtreaction": (D, [P, D, D]),
+            "oracle_rhocpfluid": (D, [P, D]),
+            "oracle_ksolid": (D, [P, D]),
+            "oracle_kfluid": (D, [P, D]),
+            "oracle_gibbs": (D, [P, D, D, D, D, D, D]),
+            "oracle_rel_enthalpy": (D, [P, D, D]),
+            "oracle_reaction_constant": (D, [P, D, D, D]),
+            "oracle_scatter_only": (None, [P, P, I64, P]),
+            "oracle_node_properties": (None, [P, P, P]),
+            "oracle_insulating_bc": (None, [P, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
