@@ -155,7 +155,8 @@ class ErebusStepStats(Structure):
 class ErebusSolverOptions(Structure):
     _fields_ = [
         ("hydro_rtol", c_double), ("thermal_rtol", c_double),
-        ("gravity_rtol", c_double), ("max_iters", c_int32), ("restart", c_int32),
+        ("gravity_rtol", c_double), ("max_refinements", c_int32),
+        ("reuse_factors", c_int32), ("direct_solver", c_int32), ("reserved", c_int32),
     ]
 
 

@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liberebus_b200.so")
-SOURCES = ["api.cu", "markers.cu", "stencils.cu", "assemble.cu", "bandlu.cu"]
+SOURCES = ["api.cu", "markers.cu", "stencils.cu", "assemble.cu", "bandlu.cu", "mfront.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -22,7 +22,7 @@ FLAGS = [
 
 def build(force=False, verbose=False):
     srcs = [os.path.join(SRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(SRC, h) for h in os.listdir(SRC) if h.endswith(".cuh")]
+    deps = srcs + [os.path.join(SRC, h) for h in os.listdir(SRC) if h.endswith((".cuh", ".h"))]
     deps.append(os.path.join(os.path.dirname(HERE), "include", "erebus_b200.h"))
     if (not force and os.path.exists(LIB)
             and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps)):

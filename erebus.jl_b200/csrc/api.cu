@@ -184,8 +184,10 @@ int erebus_default_solver_options(ErebusSolverOptions *o) {
     o->hydro_rtol = 1e-13;
     o->thermal_rtol = 1e-13;
     o->gravity_rtol = 1e-13;
-    o->max_iters = 4;
-    o->restart = 0;
+    o->max_refinements = 4;
+    o->reuse_factors = 1;
+    o->direct_solver = EREBUS_SOLVER_MULTIFRONTAL;
+    o->reserved = 0;
     return EREBUS_OK;
 }
 
@@ -300,6 +302,7 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
     std::memset(s->hsc, 0, sizeof(DevScalars));
     if (band_alloc(s, s->hydro, 6 * (int64_t)np, 6 * g.Ny1 + 2, 64, 12))
         return fail(EREBUS_ENOMEM, "hydro system");
+    s->hydro.dofs = 6;
     if (band_alloc(s, s->thermal, (int64_t)np, g.Ny1, 64, 5))
         return fail(EREBUS_ENOMEM, "thermal system");
     if (band_alloc(s, s->gravity, (int64_t)np, g.Ny1, 64, 5))
@@ -315,8 +318,12 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
 
 int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o) {
     if (!s || !o) return EREBUS_EINVAL;
+    if (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL && o->direct_solver != EREBUS_SOLVER_BAND)
+        return EREBUS_EINVAL;
+    if (o->direct_solver != s->opt.direct_solver) {   // factors of the other solver are stale
+        s->hydro.factored = s->thermal.factored = s->gravity.factored = false;
+    }
     s->opt = *o;
-    s->opt_no_reuse = o->restart < 0;
     return EREBUS_OK;
 }
 
@@ -489,7 +496,7 @@ int erebus_gravity(erebus_state *s, ErebusSolveStats *st) {
     if (!s) return EREBUS_EINVAL;
     cudaSetDevice(s->device);
     TRY(assemble_system(s, SYS_GRAVITY));
-    TRY(band_solve_refined(s, s->gravity, s->opt.gravity_rtol, s->opt.max_iters, st));
+    TRY(band_solve_refined(s, s->gravity, s->opt.gravity_rtol, s->opt.max_refinements, st));
     size_t np = (size_t)s->g.Nx1 * s->g.Ny1;
     TRY(check_cuda(s, cudaMemcpyAsync(s->grid[G_FI], s->gravity.x, np * 8,
                                       cudaMemcpyDeviceToDevice, s->stream), "FI"));
@@ -514,7 +521,7 @@ int erebus_hydromech_pass(erebus_state *s, double *dt, int32_t iplast, int32_t *
     TRY(bulk_viscosity(s));
     TRY(assemble_system(s, SYS_HYDRO));
     timer_end(s, PH_HYDRO_ASSEMBLE);
-    TRY(band_solve_refined(s, s->hydro, s->opt.hydro_rtol, s->opt.max_iters, st));
+    TRY(band_solve_refined(s, s->hydro, s->opt.hydro_rtol, s->opt.max_refinements, st));
     timer_begin(s, PH_HYDRO_POST);
     TRY(hydro_post(s, s->hydro.x));
     timer_end(s, PH_HYDRO_POST);
@@ -550,7 +557,7 @@ int erebus_thermal_solve(erebus_state *s, double dt, int32_t timestep, double *m
     timer_begin(s, PH_THERMAL_ASSEMBLE);
     TRY(assemble_system(s, SYS_THERMAL));
     timer_end(s, PH_THERMAL_ASSEMBLE);
-    TRY(band_solve_refined(s, s->thermal, s->opt.thermal_rtol, s->opt.max_iters, st));
+    TRY(band_solve_refined(s, s->thermal, s->opt.thermal_rtol, s->opt.max_refinements, st));
     TRY(thermal_post(s, s->thermal.x));
     TRY(read_scalars(s));
     s->last_maxDT = slot(s, X_DT);

@@ -16,181 +16,9 @@
 // time: on timeout the kernel records an error and runs to completion.
 #include <cooperative_groups.h>
 #include "solver.cuh"
+#include "tiles.cuh"
 
 namespace erebus {
-
-constexpr int NB_TILE = 64;       // tile size
-constexpr int LU_THREADS = 256;
-constexpr unsigned long long BARRIER_TIMEOUT_NS = 2000000000ull;   // 2 s
-
-__device__ __forceinline__ unsigned long long globaltimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Sense-reversing grid barrier over all CTAs of a cooperative launch.
-// bar[0] = arrival count, bar[1] = generation.  A wait that exceeds the
-// timeout sets *err and returns.
-__device__ void grid_barrier(unsigned int *bar, int *err) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int *vgen = bar + 1;
-        unsigned int gen = *vgen;
-        __threadfence();
-        unsigned int arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned long long t0 = globaltimer();
-            while (*vgen == gen) {
-                if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
-                    atomicExch(err, 1);
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
-// tile primitives (one CTA of 256 threads, 64 x 64 FP64 tiles)
-//
-// Register layout of a tile held by the CTA: thread (ty, tx) = (tid/16,
-// tid%16) owns rows r = ty + 16 i and columns c = tx + 16 j, i, j = 0..3.
-// Shared-memory tiles are column-major with leading dimension LDS = 65
-// (conflict-free staging).  Data another CTA wrote during this kernel is
-// read with ld.global.cg (L2), never through the non-coherent L1.
-// ---------------------------------------------------------------------------
-constexpr int LDS = NB_TILE + 1;
-constexpr int STILE = NB_TILE * LDS;            // doubles per staged tile
-
-__device__ __forceinline__ void fence_proxy_async() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// global column-major tile -> smem column-major (ld LDS)
-__device__ __forceinline__ void stage_tile(double *dst, const double *src) {
-    const double2 *s2 = reinterpret_cast<const double2 *>(src);
-    double2 v[8];
-#pragma unroll
-    for (int q = 0; q < 8; q++) v[q] = __ldcg(&s2[threadIdx.x + 256 * q]);
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        int e = 2 * (threadIdx.x + 256 * q), r = e % NB_TILE, c = e / NB_TILE;
-        dst[c * LDS + r] = v[q].x;
-        dst[c * LDS + r + 1] = v[q].y;
-    }
-}
-// global column-major tile -> smem transposed (Bt[k*LDS + c] = B(k, c))
-__device__ __forceinline__ void stage_tile_t(double *dst, const double *src) {
-    const double2 *s2 = reinterpret_cast<const double2 *>(src);
-    double2 v[8];
-#pragma unroll
-    for (int q = 0; q < 8; q++) v[q] = __ldcg(&s2[threadIdx.x + 256 * q]);
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        int e = 2 * (threadIdx.x + 256 * q), k = e % NB_TILE, c = e / NB_TILE;
-        dst[k * LDS + c] = v[q].x;
-        dst[(k + 1) * LDS + c] = v[q].y;
-    }
-}
-// smem column-major (ld LDS) -> global column-major
-__device__ __forceinline__ void unstage_tile(double *dst, const double *src) {
-    double2 *d2 = reinterpret_cast<double2 *>(dst);
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        int e = 2 * (threadIdx.x + 256 * q), r = e % NB_TILE, c = e / NB_TILE;
-        d2[threadIdx.x + 256 * q] = make_double2(src[c * LDS + r], src[c * LDS + r + 1]);
-    }
-}
-__device__ __forceinline__ void regs_from_smem(const double *S, double a[4][4]) {
-    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) a[i][j] = S[(tx + 16 * j) * LDS + ty + 16 * i];
-}
-__device__ __forceinline__ void regs_to_smem(double *S, const double a[4][4]) {
-    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) S[(tx + 16 * j) * LDS + ty + 16 * i] = a[i][j];
-}
-// acc (+)= A * B with As column-major (ld LDS) and Bt transposed (ld LDS)
-__device__ __forceinline__ void gemm_acc(const double *As, const double *Bt, double acc[4][4]) {
-    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-#pragma unroll 4
-    for (int k = 0; k < NB_TILE; k++) {
-        double av[4], bv[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) av[i] = As[k * LDS + ty + 16 * i];
-#pragma unroll
-        for (int j = 0; j < 4; j++) bv[j] = Bt[k * LDS + tx + 16 * j];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
-    }
-}
-
-// In-place Gauss-Jordan inverse (no pivoting) of the tile held in registers
-// `a` (the layout above): step k publishes column k and row k, then every
-// thread updates its 16 elements branch-free; one barrier per step
-// (broadcast vectors double-buffered).  A zero or non-finite pivot raises
-// *err = 2.
-__device__ void tile_inverse(double a[4][4], double *vec, int *err) {
-    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-#pragma unroll
-    for (int kq = 0; kq < 4; kq++)
-        for (int kk = 0; kk < 16; kk++) {
-            const int k = kq * 16 + kk;
-            double *col = vec + (k & 1) * 2 * NB_TILE, *row = col + NB_TILE;
-            if (tx == kk) {
-#pragma unroll
-                for (int i = 0; i < 4; i++) col[ty + 16 * i] = a[i][kq];
-            }
-            if (ty == kk) {
-#pragma unroll
-                for (int j = 0; j < 4; j++) row[tx + 16 * j] = a[kq][j];
-            }
-            __syncthreads();
-            double piv = row[k];
-            if (threadIdx.x == 0 && !(fabs(piv) > 0.0 && fabs(piv) < INFINITY)) atomicExch(err, 2);
-            double ip = 1.0 / piv;
-            double f[4], rk[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) f[i] = col[ty + 16 * i] * ip;
-#pragma unroll
-            for (int j = 0; j < 4; j++) rk[j] = row[tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) a[i][j] = fma(-f[i], rk[j], a[i][j]);
-            // column k (rows != k), then row k, then the pivot
-            if (tx == kk) {
-#pragma unroll
-                for (int i = 0; i < 4; i++) a[i][kq] = -f[i];
-            }
-            if (ty == kk) {
-#pragma unroll
-                for (int j = 0; j < 4; j++) a[kq][j] = rk[j] * ip;
-                if (tx == kk) a[kq][kq] = ip;
-            }
-        }
-    __syncthreads();
-}
-
-struct FactorSmem {
-    double As[STILE], Bt[STILE], Cs[STILE];
-    double vec[2 * 2 * NB_TILE];
-};
 
 // Invert diagonal tile (K,K), whose updated values are in registers `a`,
 // and store the inverse in its place.
@@ -641,8 +469,6 @@ BandView band_view(BandSystem &sys) {
     B.rhs = sys.rhs;
     B.rscale = sys.rscale;
     B.x = sys.x;
-    B.invL = sys.invL;
-    B.invU = sys.invU;
     B.ell_cols = sys.ell_cols;
     B.ell_vals = sys.ell_vals;
     return B;
@@ -661,11 +487,7 @@ int band_alloc(erebus_state *s, BandSystem &sys, int64_t n, int b, int nb, int e
     sys.Bb = (b + NB_TILE - 1) / NB_TILE;
     sys.ell = ell;
     int64_t np = (int64_t)sys.NB * sys.nb;
-    size_t t2 = (size_t)NB_TILE * NB_TILE * sizeof(double);
-    cudaError_t e = cudaMalloc(&sys.tiles, tiles_bytes(sys));
-    if (e == cudaSuccess) e = cudaMalloc(&sys.invL, sys.NB * t2);
-    if (e == cudaSuccess) e = cudaMalloc(&sys.invU, sys.NB * t2);
-    if (e == cudaSuccess) e = cudaMalloc(&sys.rscale, np * 8);
+    cudaError_t e = cudaMalloc(&sys.rscale, np * 8);
     if (e == cudaSuccess) e = cudaMalloc(&sys.rhs, np * 8);
     if (e == cudaSuccess) e = cudaMalloc(&sys.x, np * 8);
     if (e == cudaSuccess) e = cudaMalloc(&sys.r, np * 8);
@@ -687,8 +509,21 @@ int band_alloc(erebus_state *s, BandSystem &sys, int64_t n, int b, int nb, int e
     return EREBUS_OK;
 }
 
+// The band storage of the band LU, allocated on first use.
+static int band_tiles(erebus_state *s, BandSystem &sys) {
+    if (sys.tiles) return EREBUS_OK;
+    cudaError_t e = cudaMalloc(&sys.tiles, tiles_bytes(sys));
+    if (e != cudaSuccess) {
+        sys.tiles = nullptr;
+        s->last_error = std::string("band storage: ") + cudaGetErrorString(e);
+        return EREBUS_ENOMEM;
+    }
+    return EREBUS_OK;
+}
+
 int band_free(BandSystem &sys) {
-    void *ps[] = {sys.tiles, sys.invL, sys.invU, sys.rscale, sys.rhs, sys.x, sys.r,
+    mf_release(sys);
+    void *ps[] = {sys.tiles, sys.rscale, sys.rhs, sys.x, sys.r,
                   sys.d, sys.ell_vals, sys.ell_cols, sys.ell_prev, sys.changed,
                   sys.bar, sys.err};
     for (void *p : ps)
@@ -698,6 +533,8 @@ int band_free(BandSystem &sys) {
 }
 
 int band_zero(erebus_state *s, BandSystem &sys) {
+    int rc = band_tiles(s, sys);
+    if (rc) return rc;
     return check_cuda(s, cudaMemsetAsync(sys.tiles, 0, tiles_bytes(sys), s->stream),
                       "band_zero");
 }
@@ -719,14 +556,25 @@ static int lu_error(erebus_state *s, BandSystem &sys, const char *what) {
     if (rc) return rc;
     if (h) {
         s->last_error = std::string(what) +
-                        (h == 1 ? ": grid barrier timed out" : ": zero pivot");
+                        (h == 1 ? ": grid barrier timed out"
+                         : h == 2 ? ": zero pivot"
+                         : h == 3 ? ": wait timed out"
+                                  : ": matrix pattern changed since the analysis");
         cudaMemsetAsync(sys.err, 0, sizeof(int), s->stream);
-        return h == 1 ? EREBUS_ECUDA : EREBUS_ENOCONV;
+        if (h == 4) mf_release(sys);   // analysed again at the next factorisation
+        return h == 2 ? EREBUS_ENOCONV : EREBUS_ECUDA;
     }
     return EREBUS_OK;
 }
 
+bool use_multifrontal(const erebus_state *s) {
+    return s->opt.direct_solver != EREBUS_SOLVER_BAND;
+}
+
 int band_factor(erebus_state *s, BandSystem &sys) {
+    if (use_multifrontal(s)) return mf_factor(s, sys);
+    int trc = band_tiles(s, sys);
+    if (trc) return trc;
     size_t smem = sizeof(FactorSmem);
     cudaFuncSetAttribute(k_band_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
@@ -753,6 +601,7 @@ int band_factor(erebus_state *s, BandSystem &sys) {
 
 // In-place solve L U w = w with the cluster kernel.
 static int band_solve_inplace(erebus_state *s, BandSystem &sys, double *w) {
+    if (use_multifrontal(s)) return mf_solve(s, sys, w);
     if (sys.Bb > 2 * SOLVE_P) {
         s->last_error = "band_solve: band too wide for the cluster solve";
         return EREBUS_EINVAL;

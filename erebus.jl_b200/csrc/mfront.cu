@@ -1,0 +1,641 @@
+// mfront.cu -- nested-dissection multifrontal LU of the row-scaled systems.
+//
+// The reference factorises each system with a sparse direct LU (UMFPACK,
+// E:6612, E:6736-6748, E:6925).  Here the unknowns are ordered by nested
+// dissection of the P-node grid (mf_plan.h) and the LU runs front by front,
+// level by level from the leaves to the root, without pivoting:
+//
+//   assembly   the scaled ELL entries are stored into the fronts that
+//              eliminate them (k_mf_scatter), padding unknowns become
+//              identity rows (k_mf_pad);
+//   factor     (k_mf_factor, one persistent cooperative kernel) per level:
+//              extend-add of the children's Schur complements, then for each
+//              64-column block K of the eliminated part the inverse of the
+//              diagonal tile D_K (Gauss-Jordan), L_IK = A_IK D_K^{-1}, and
+//              the rank-64 update of the eliminated rows and columns; last
+//              the Schur complement of the update block with inner dimension
+//              Kp (tile GEMMs, FP64 FMA);
+//   solve      (k_mf_solve) forward over the levels from the leaves, backward
+//              from the root; each front gathers its children's update
+//              vectors and its ring solution through index maps.
+//
+// Levels with many small fronts run one front per CTA with no grid barrier
+// inside; levels with few large fronts spread each step's tile tasks over
+// all CTAs, separated by the bounded grid barrier.  Results do not depend
+// on the number of CTAs: every tile is computed by one CTA in a fixed order.
+#include <cooperative_groups.h>
+
+#include <vector>
+
+#include "mf_plan.h"
+#include "solver.cuh"
+#include "tiles.cuh"
+
+namespace erebus {
+
+constexpr int T2 = NB_TILE * NB_TILE;
+static_assert(MF_TILE == NB_TILE, "front tiles are the LU tiles");
+
+struct MfView {
+    const MfFront *fr;
+    double *F;          // front storage
+    double *vec;        // front vectors (solve)
+    const int *vars;    // local -> global unknown
+    const int *eamap;   // local -> children's update index
+    const int *lvl;     // level ranges (nlev + 1)
+    const int *lvl_kt;  // max Kt per level
+    int nlev;
+    const long long *target;   // ELL entry -> storage offset
+    const int *expect;         // ELL column pattern the targets were built from
+    long long n;
+    int ell;
+};
+
+struct MfDevice {
+    MfPlan plan;
+    MfFront *fr = nullptr;
+    double *F = nullptr, *vec = nullptr;
+    int *vars = nullptr, *eamap = nullptr, *lvl = nullptr, *lvl_kt = nullptr;
+    long long *target = nullptr;
+    int *expect = nullptr;
+    int nlev = 0;
+};
+
+__device__ __forceinline__ double *ftile(const MfView &V, const MfFront &f, int I, int J) {
+    return V.F + f.off + ((long long)J * f.Mt + I) * T2;
+}
+__device__ __forceinline__ long long felem(const MfFront &f, int a, int b) {
+    return f.off + ((long long)(b >> 6) * f.Mt + (a >> 6)) * T2 + (b & 63) * 64 + (a & 63);
+}
+
+// ---------------------------------------------------------------------------
+// assembly
+// ---------------------------------------------------------------------------
+__global__ void k_mf_scatter(MfView V, const int *cols, const double *vals, int *err) {
+    long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= V.n) return;
+    for (int s = 0; s < V.ell; s++) {
+        long long e = row * V.ell + s;
+        int c = cols[e];
+        if (c != V.expect[e]) {
+            atomicExch(err, 4);
+            continue;
+        }
+        long long t = V.target[e];
+        if (t >= 0) V.F[t] += vals[e];
+    }
+}
+
+__global__ void k_mf_pad(MfView V, int nfronts) {
+    int f = blockIdx.x;
+    if (f >= nfronts) return;
+    MfFront fr = V.fr[f];
+    for (int a = fr.k + threadIdx.x; a < fr.Kp; a += blockDim.x) V.F[felem(fr, a, a)] = 1.0;
+}
+
+// ---------------------------------------------------------------------------
+// factor: CTA-wide tile operations (FactorSmem staging, 256 threads)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void negate(double a[4][4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) a[i][j] = -a[i][j];
+}
+
+// Tile (I, J) of front f += the children's Schur complement entries that
+// map onto it (child 0 first, then child 1).
+__device__ void mf_extend_add_tile(const MfView &V, const MfFront &f, int I, int J) {
+    double *T = ftile(V, f, I, J);
+    const int *map = V.eamap + f.map_off;
+    MfFront C0, C1;
+    bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
+    if (h0) C0 = V.fr[f.c0];
+    if (h1) C1 = V.fr[f.c1];
+#pragma unroll 4
+    for (int q = 0; q < 16; q++) {
+        int e = threadIdx.x + 256 * q, r = e & 63, c = e >> 6;
+        int a = I * 64 + r, b = J * 64 + c;
+        double s = __ldcg(&T[c * 64 + r]);
+        if (h0) {
+            int ia = __ldg(&map[2 * a]), ib = __ldg(&map[2 * b]);
+            if (ia >= 0 && ib >= 0) s += __ldcg(V.F + felem(C0, C0.Kp + ia, C0.Kp + ib));
+        }
+        if (h1) {
+            int ia = __ldg(&map[2 * a + 1]), ib = __ldg(&map[2 * b + 1]);
+            if (ia >= 0 && ib >= 0) s += __ldcg(V.F + felem(C1, C1.Kp + ia, C1.Kp + ib));
+        }
+        T[c * 64 + r] = s;
+    }
+}
+
+__device__ void mf_invert_tile(double *T, FactorSmem &S, int *err) {
+    double a[4][4];
+    stage_tile(S.Cs, T);
+    __syncthreads();
+    regs_from_smem(S.Cs, a);
+    __syncthreads();
+    tile_inverse(a, S.vec, err);
+    regs_to_smem(S.Cs, a);
+    __syncthreads();
+    unstage_tile(T, S.Cs);
+    __syncthreads();
+}
+
+// L_IK = A_IK D_K^{-1} (tile (K,K) holds D_K^{-1})
+__device__ void mf_l_tile(const MfView &V, const MfFront &f, int I, int K, FactorSmem &S) {
+    double acc[4][4] = {};
+    double *T = ftile(V, f, I, K);
+    stage_tile(S.As, T);
+    stage_tile_t(S.Bt, ftile(V, f, K, K));
+    __syncthreads();
+    gemm_acc(S.As, S.Bt, acc);
+    regs_to_smem(S.Cs, acc);
+    __syncthreads();
+    unstage_tile(T, S.Cs);
+    __syncthreads();
+}
+
+// A_IJ -= sum_{K in [k0, k1)} L_IK A_KJ; optionally invert the result.
+__device__ void mf_update_tile(const MfView &V, const MfFront &f, int I, int J, int k0,
+                               int k1, FactorSmem &S, int *err, bool invert) {
+    double acc[4][4];
+    double *C = ftile(V, f, I, J);
+    stage_tile(S.Cs, C);
+    __syncthreads();
+    regs_from_smem(S.Cs, acc);
+    negate(acc);
+    for (int K = k0; K < k1; K++) {
+        __syncthreads();
+        stage_tile(S.As, ftile(V, f, I, K));
+        stage_tile_t(S.Bt, ftile(V, f, K, J));
+        __syncthreads();
+        gemm_acc(S.As, S.Bt, acc);
+    }
+    negate(acc);
+    __syncthreads();
+    if (invert) tile_inverse(acc, S.vec, err);
+    regs_to_smem(S.Cs, acc);
+    __syncthreads();
+    unstage_tile(C, S.Cs);
+    __syncthreads();
+}
+
+// Number of update tasks of step K: rows/cols K+1..Mt-1 except the block
+// of update rows and update columns (deferred to the Schur phase).
+__device__ __forceinline__ int mf_nupd(const MfFront &f, int K) {
+    if (K >= f.Kt) return 0;
+    int R = f.Mt - K - 1, e = f.Kt - K - 1;
+    return e * R + (f.Mt - f.Kt) * e;
+}
+__device__ __forceinline__ void mf_upd_ij(const MfFront &f, int K, int u, int &I, int &J) {
+    int R = f.Mt - K - 1, e = f.Kt - K - 1;
+    if (u < e * R) {           // eliminated rows, all columns
+        I = K + 1 + u % e;
+        J = K + 1 + u / e;
+    } else {                   // update rows, eliminated columns
+        u -= e * R;
+        int ru = f.Mt - f.Kt;
+        I = f.Kt + u % ru;
+        J = K + 1 + u / ru;
+    }
+}
+
+// The whole partial LU of one front by one CTA.
+__device__ void mf_factor_local(const MfView &V, const MfFront &f, FactorSmem &S, int *err) {
+    if (f.c0 >= 0 || f.c1 >= 0) {
+        for (int t = 0; t < f.Mt * f.Mt; t++) mf_extend_add_tile(V, f, t % f.Mt, t / f.Mt);
+        __threadfence_block();
+        __syncthreads();
+    }
+    for (int K = 0; K < f.Kt; K++) {
+        if (K == 0) mf_invert_tile(ftile(V, f, 0, 0), S, err);
+        for (int I = K + 1; I < f.Mt; I++) mf_l_tile(V, f, I, K, S);
+        int nu = mf_nupd(f, K);
+        for (int u = 0; u < nu; u++) {
+            int I, J;
+            mf_upd_ij(f, K, u, I, J);
+            mf_update_tile(V, f, I, J, K, K + 1, S, err, I == K + 1 && J == K + 1);
+        }
+    }
+    for (int J = f.Kt; J < f.Mt; J++)
+        for (int I = f.Kt; I < f.Mt; I++) mf_update_tile(V, f, I, J, 0, f.Kt, S, err, false);
+}
+
+// Runs task(f, u) for the tasks u in [0, count(f)) of the fronts [fb, fe),
+// numbered consecutively across the fronts and dealt round-robin to CTAs.
+template <class Count, class Task>
+__device__ void mf_for_tasks(const MfView &V, int fb, int fe, Count count, Task task) {
+    const int G = gridDim.x, me = blockIdx.x;
+    long long base = 0;
+    for (int fi = fb; fi < fe; fi++) {
+        const MfFront f = V.fr[fi];
+        int cnt = count(f);
+        if (cnt <= 0) continue;
+        int first = (int)(((me - base) % G + G) % G);
+        for (int u = first; u < cnt; u += G) task(f, u);
+        base += cnt;
+    }
+}
+
+__global__ void __launch_bounds__(LU_THREADS, 2)
+k_mf_factor(MfView V, unsigned int *bar, int *err) {
+    extern __shared__ __align__(16) double smem_raw[];
+    FactorSmem &S = *reinterpret_cast<FactorSmem *>(smem_raw);
+    const int G = gridDim.x;
+    for (int p = 0; p < V.nlev; p++) {
+        const int fb = V.lvl[p], fe = V.lvl[p + 1];
+        if (fe - fb >= G / 2) {
+            for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
+                const MfFront f = V.fr[fi];
+                mf_factor_local(V, f, S, err);
+            }
+            grid_barrier(bar, err);
+            continue;
+        }
+        // extend-add; the task of tile (0,0) also inverts it
+        mf_for_tasks(
+            V, fb, fe, [](const MfFront &f) { return f.Mt * f.Mt; },
+            [&](const MfFront &f, int u) {
+                int I = u % f.Mt, J = u / f.Mt;
+                if (f.c0 >= 0 || f.c1 >= 0) {
+                    mf_extend_add_tile(V, f, I, J);
+                    __syncthreads();
+                }
+                if (u == 0 && f.Kt > 0) mf_invert_tile(ftile(V, f, 0, 0), S, err);
+            });
+        grid_barrier(bar, err);
+        const int ktmax = V.lvl_kt[p];
+        for (int K = 0; K < ktmax; K++) {
+            mf_for_tasks(
+                V, fb, fe, [K](const MfFront &f) { return K < f.Kt ? f.Mt - K - 1 : 0; },
+                [&](const MfFront &f, int u) { mf_l_tile(V, f, K + 1 + u, K, S); });
+            grid_barrier(bar, err);
+            mf_for_tasks(
+                V, fb, fe, [K](const MfFront &f) { return mf_nupd(f, K); },
+                [&](const MfFront &f, int u) {
+                    int I, J;
+                    mf_upd_ij(f, K, u, I, J);
+                    mf_update_tile(V, f, I, J, K, K + 1, S, err, I == K + 1 && J == K + 1);
+                });
+            grid_barrier(bar, err);
+        }
+        mf_for_tasks(
+            V, fb, fe, [](const MfFront &f) { return (f.Mt - f.Kt) * (f.Mt - f.Kt); },
+            [&](const MfFront &f, int u) {
+                int ru = f.Mt - f.Kt;
+                mf_update_tile(V, f, f.Kt + u % ru, f.Kt + u / ru, 0, f.Kt, S, err, false);
+            });
+        grid_barrier(bar, err);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// solve
+// ---------------------------------------------------------------------------
+struct MfSolveSmem {
+    double x[8][64];       // per-warp vector pieces
+    double part[8][64];    // per-warp partial sums
+    double y[64];
+};
+
+// lane's rows r0 = lane, r1 = lane + 32 of T x (T a 64 x 64 column-major
+// tile in global memory, x in shared memory)
+__device__ __forceinline__ void warp_tile_gemv(const double *T, const double *x, double &s0,
+                                               double &s1) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll 8
+    for (int c = 0; c < 64; c++) {
+        double xc = x[c];
+        s0 = fma(__ldcg(&T[c * 64 + lane]), xc, s0);
+        s1 = fma(__ldcg(&T[c * 64 + lane + 32]), xc, s1);
+    }
+}
+
+// v[I] -= sum_{K in ks} T(I, K) v[K] for one target tile row I, the K range
+// split over the 8 warps, partial sums reduced through shared memory.
+// `xsrc(K, c)` gives element c of the vector piece K.
+template <class Xsrc>
+__device__ void mf_row_gemv(const MfView &V, const MfFront &f, double *v, int I, int k0, int k1,
+                            Xsrc xsrc, MfSolveSmem &S) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double s0 = 0.0, s1 = 0.0;
+    for (int K = k0 + w; K < k1; K += 8) {
+        S.x[w][lane] = xsrc(K, lane);
+        S.x[w][lane + 32] = xsrc(K, lane + 32);
+        __syncwarp();
+        warp_tile_gemv(ftile(V, f, I, K), S.x[w], s0, s1);
+        __syncwarp();
+    }
+    S.part[w][lane] = s0;
+    S.part[w][lane + 32] = s1;
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) s += S.part[q][threadIdx.x];
+        double *d = &v[I * 64 + threadIdx.x];
+        __stcg(d, __ldcg(d) - s);
+    }
+    __syncthreads();
+}
+
+// Gathers the front vector: the right-hand side of the eliminated unknowns
+// plus the children's update vectors.
+__device__ void mf_gather_fwd(const MfView &V, const MfFront &f, const double *w, double *v) {
+    const int *var = V.vars + f.var_off, *map = V.eamap + f.map_off;
+    MfFront C0, C1;
+    bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
+    if (h0) C0 = V.fr[f.c0];
+    if (h1) C1 = V.fr[f.c1];
+    for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
+        int g = var[a];
+        double s = (a < f.Kp && g >= 0) ? __ldcg(&w[g]) : 0.0;
+        if (h0) {
+            int i = map[2 * a];
+            if (i >= 0) s += __ldcg(&V.vec[C0.vec_off + C0.Kp + i]);
+        }
+        if (h1) {
+            int i = map[2 * a + 1];
+            if (i >= 0) s += __ldcg(&V.vec[C1.vec_off + C1.Kp + i]);
+        }
+        __stcg(&v[a], s);
+    }
+}
+
+// Forward elimination inside the front: for K < Kt, rows I in (K, iend)
+// get v_I -= L_IK v_K; the warps take different rows.
+__device__ void mf_fwd_front(const MfView &V, const MfFront &f, double *v, int iend,
+                             MfSolveSmem &S) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int K = 0; K < f.Kt; K++) {
+        if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
+        __syncthreads();
+        for (int I = K + 1 + w; I < iend; I += 8) {
+            double s0 = 0.0, s1 = 0.0;
+            warp_tile_gemv(ftile(V, f, I, K), S.y, s0, s1);
+            double *d = &v[I * 64];
+            __stcg(&d[lane], __ldcg(&d[lane]) - s0);
+            __stcg(&d[lane + 32], __ldcg(&d[lane + 32]) - s1);
+        }
+        __syncthreads();
+    }
+}
+
+// Backward substitution inside the front (the update part already
+// subtracted): x_K = D_K^{-1} v_K, then v_I -= U_IK x_K for I < K; the
+// solution goes to v and to w.
+__device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, double *wout,
+                             MfSolveSmem &S) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int *var = V.vars + f.var_off;
+    for (int K = f.Kt - 1; K >= 0; K--) {
+        if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
+        __syncthreads();
+        // x_K = D^{-1} y: four column quarters per row, reduced in part
+        {
+            const double *Di = ftile(V, f, K, K);
+            int r = threadIdx.x & 63, q = threadIdx.x >> 6;
+            double s = 0.0;
+#pragma unroll 4
+            for (int c = q * 16; c < q * 16 + 16; c++) s = fma(__ldcg(&Di[c * 64 + r]), S.y[c], s);
+            S.part[q][r] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x < 64) {
+            int r = threadIdx.x;
+            double x = (S.part[0][r] + S.part[1][r]) + (S.part[2][r] + S.part[3][r]);
+            S.x[0][r] = x;
+            __stcg(&v[K * 64 + r], x);
+            int a = K * 64 + r;
+            if (a < f.k) __stcg(&wout[var[a]], x);
+        }
+        __syncthreads();
+        for (int I = w; I < K; I += 8) {
+            double s0 = 0.0, s1 = 0.0;
+            warp_tile_gemv(ftile(V, f, I, K), S.x[0], s0, s1);
+            double *d = &v[I * 64];
+            __stcg(&d[lane], __ldcg(&d[lane]) - s0);
+            __stcg(&d[lane + 32], __ldcg(&d[lane + 32]) - s1);
+        }
+        __syncthreads();
+    }
+}
+
+// Solves L U x = w in place (w: n values; rows >= n untouched).
+__global__ void __launch_bounds__(LU_THREADS, 2)
+k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
+    __shared__ MfSolveSmem S;
+    const int G = gridDim.x;
+    // forward: leaves to root
+    for (int p = 0; p < V.nlev; p++) {
+        const int fb = V.lvl[p], fe = V.lvl[p + 1];
+        const bool local = fe - fb >= G / 2;
+        for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
+            const MfFront f = V.fr[fi];
+            double *v = V.vec + f.vec_off;
+            mf_gather_fwd(V, f, w, v);
+            __syncthreads();
+            mf_fwd_front(V, f, v, local ? f.Mt : f.Kt, S);
+        }
+        if (!local) {
+            grid_barrier(bar, err);
+            // update rows: v_I -= sum_{K < Kt} L_IK y_K
+            mf_for_tasks(
+                V, fb, fe, [](const MfFront &f) { return f.Mt - f.Kt; },
+                [&](const MfFront &f, int u) {
+                    double *v = V.vec + f.vec_off;
+                    mf_row_gemv(V, f, v, f.Kt + u, 0, f.Kt,
+                                [&](int K, int c) { return __ldcg(&v[K * 64 + c]); }, S);
+                });
+        }
+        grid_barrier(bar, err);
+    }
+    // backward: root to leaves
+    for (int p = V.nlev - 1; p >= 0; p--) {
+        const int fb = V.lvl[p], fe = V.lvl[p + 1];
+        const bool local = fe - fb >= G / 2;
+        auto ring_x = [&](const MfFront &f) {
+            const int *var = V.vars + f.var_off;
+            return [=](int J, int c) {
+                int g = var[J * 64 + c];
+                return g >= 0 ? __ldcg(&w[g]) : 0.0;
+            };
+        };
+        if (!local) {
+            // eliminated rows: v_K -= sum_{J >= Kt} U_KJ x_J
+            mf_for_tasks(
+                V, fb, fe, [](const MfFront &f) { return f.Mt > f.Kt ? f.Kt : 0; },
+                [&](const MfFront &f, int u) {
+                    mf_row_gemv(V, f, V.vec + f.vec_off, u, f.Kt, f.Mt, ring_x(f), S);
+                });
+            grid_barrier(bar, err);
+        }
+        for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
+            const MfFront f = V.fr[fi];
+            double *v = V.vec + f.vec_off;
+            if (local)
+                for (int K = 0; K < f.Kt && f.Mt > f.Kt; K++)
+                    mf_row_gemv(V, f, v, K, f.Kt, f.Mt, ring_x(f), S);
+            mf_bwd_front(V, f, v, w, S);
+        }
+        grid_barrier(bar, err);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
+    MfView V;
+    V.fr = D.fr;
+    V.F = D.F;
+    V.vec = D.vec;
+    V.vars = D.vars;
+    V.eamap = D.eamap;
+    V.lvl = D.lvl;
+    V.lvl_kt = D.lvl_kt;
+    V.nlev = D.nlev;
+    V.target = D.target;
+    V.expect = D.expect;
+    V.n = sys.n;
+    V.ell = sys.ell;
+    return V;
+}
+
+void mf_release(BandSystem &sys) {
+    MfDevice *D = sys.mf;
+    if (!D) return;
+    void *ps[] = {D->fr, D->F, D->vec, D->vars, D->eamap, D->lvl, D->lvl_kt, D->target,
+                  D->expect};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    delete D;
+    sys.mf = nullptr;
+}
+
+template <class T>
+static cudaError_t upload(T **dst, const std::vector<T> &src, cudaStream_t st) {
+    cudaError_t e = cudaMalloc(dst, std::max<size_t>(1, src.size()) * sizeof(T));
+    if (e == cudaSuccess && !src.empty())
+        e = cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+    return e;
+}
+
+// Builds the plan of `sys` from the column pattern of its assembled ELL
+// matrix (on the device) and uploads it.
+static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
+    mf_release(sys);
+    MfDevice *D = new MfDevice();
+    sys.mf = D;
+    int64_t rows = (int64_t)sys.NB * sys.nb;
+    std::vector<int> cols(rows * sys.ell);
+    int rc = check_cuda(s, cudaMemcpyAsync(cols.data(), sys.ell_cols, cols.size() * 4,
+                                           cudaMemcpyDeviceToHost, s->stream), "mf pattern");
+    if (!rc) rc = check_cuda(s, cudaStreamSynchronize(s->stream), "mf pattern");
+    if (rc) return rc;
+    MfPlan &P = D->plan;
+    // leaves of 16 nodes for the 6-unknown system (96 unknowns), 64 nodes
+    // for the scalar ones, so a leaf fills its 64-wide tiles
+    const int leaf = dofs >= 4 ? 16 : 64;
+    if (!mf_analyse(P, dofs, s->g.Ny1, s->g.Nx1, leaf) || P.n != sys.n) {
+        s->last_error = "multifrontal analysis failed";
+        return EREBUS_EINVAL;
+    }
+    std::vector<long long> target;
+    if (!mf_targets(P, cols.data(), rows, sys.ell, target)) {
+        s->last_error = "multifrontal analysis: matrix pattern outside the fronts";
+        return EREBUS_EINVAL;
+    }
+    std::vector<int> expect(cols.begin(), cols.begin() + sys.n * sys.ell);
+    target.resize(sys.n * sys.ell);
+    std::vector<int> lvl_kt;
+    for (size_t p = 0; p + 1 < P.level_begin.size(); p++) {
+        int m = 0;
+        for (int f = P.level_begin[p]; f < P.level_begin[p + 1]; f++) m = std::max(m, P.fronts[f].Kt);
+        lvl_kt.push_back(m);
+    }
+    D->nlev = (int)P.level_begin.size() - 1;
+    cudaError_t e = upload(&D->fr, P.fronts, s->stream);
+    if (e == cudaSuccess) e = upload(&D->vars, P.vars, s->stream);
+    if (e == cudaSuccess) e = upload(&D->eamap, P.eamap, s->stream);
+    if (e == cudaSuccess) e = upload(&D->lvl, P.level_begin, s->stream);
+    if (e == cudaSuccess) e = upload(&D->lvl_kt, lvl_kt, s->stream);
+    if (e == cudaSuccess) e = upload(&D->target, target, s->stream);
+    if (e == cudaSuccess) e = upload(&D->expect, expect, s->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&D->F, P.storage * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&D->vec, P.vec * sizeof(double));
+    if (e != cudaSuccess) {
+        s->last_error = std::string("multifrontal allocation: ") + cudaGetErrorString(e);
+        return EREBUS_ENOMEM;
+    }
+    return check_cuda(s, cudaStreamSynchronize(s->stream), "mf upload");
+}
+
+static int mf_blocks(erebus_state *s, const void *func, size_t smem) {
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, LU_THREADS, smem);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    return std::min(per_sm, 2) * sms;
+}
+
+int mf_factor(erebus_state *s, BandSystem &sys) {
+    int rc;
+    if (!sys.mf) {
+        rc = mf_prepare(s, sys, sys.dofs);
+        if (rc) return rc;
+    }
+    MfDevice &D = *sys.mf;
+    MfView V = mf_view(D, sys);
+    rc = check_cuda(s, cudaMemsetAsync(D.F, 0, D.plan.storage * sizeof(double), s->stream),
+                    "mf zero");
+    if (rc) return rc;
+    EREBUS_LAUNCH(s, k_mf_scatter, nblocks(sys.n), kThreads, 0, V, sys.ell_cols, sys.ell_vals,
+                  sys.err);
+    int nf = (int)D.plan.fronts.size();
+    EREBUS_LAUNCH(s, k_mf_pad, nf, 64, 0, V, nf);
+    size_t smem = sizeof(FactorSmem);
+    cudaFuncSetAttribute(k_mf_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int blocks = mf_blocks(s, (const void *)k_mf_factor, smem);
+    if (blocks < 1) {
+        s->last_error = "mf_factor: kernel does not fit";
+        return EREBUS_ECUDA;
+    }
+    unsigned int *bar = sys.bar;
+    int *err = sys.err;
+    void *args[] = {&V, &bar, &err};
+    cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
+    rc = check_cuda(s, cudaLaunchCooperativeKernel((const void *)k_mf_factor, blocks,
+                                                   LU_THREADS, args, smem, s->stream),
+                    "mf_factor launch");
+    s->launches++;
+    if (rc) return rc;
+    sys.factored = true;
+    sys.factorizations++;
+    return EREBUS_OK;
+}
+
+int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
+    if (!sys.mf) {
+        s->last_error = "mf_solve: system not factored";
+        return EREBUS_EINVAL;
+    }
+    MfDevice &D = *sys.mf;
+    MfView V = mf_view(D, sys);
+    int blocks = mf_blocks(s, (const void *)k_mf_solve, 0);
+    if (blocks < 1) {
+        s->last_error = "mf_solve: kernel does not fit";
+        return EREBUS_ECUDA;
+    }
+    unsigned int *bar = sys.bar;
+    int *err = sys.err;
+    void *args[] = {&V, &w, &bar, &err};
+    cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
+    int rc = check_cuda(s, cudaLaunchCooperativeKernel((const void *)k_mf_solve, blocks,
+                                                       LU_THREADS, args, 0, s->stream),
+                        "mf_solve launch");
+    s->launches++;
+    return rc;
+}
+
+}  // namespace erebus

@@ -23,7 +23,6 @@ struct BandView {
     int64_t n;
     int nb, NB, Bb, ell;
     double *tiles, *rhs, *rscale, *x;
-    double *invL, *invU;     // inverses of the diagonal tiles' factors
     int *ell_cols;
     double *ell_vals;
 };
@@ -53,6 +52,13 @@ int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir
 // y = A x with the assembled (unscaled) entries
 int band_apply_unscaled(erebus_state *s, BandSystem &sys, const double *x, double *y);
 int assemble_system(erebus_state *s, int kind);
+// Nested-dissection multifrontal LU (mfront.cu): factor the assembled ELL
+// matrix of `sys`, solve in place, release the factor storage.
+int mf_factor(erebus_state *s, BandSystem &sys);
+int mf_solve(erebus_state *s, BandSystem &sys, double *w);
+void mf_release(BandSystem &sys);
+// true when `sys` is factored by the multifrontal LU (else the band LU)
+bool use_multifrontal(const erebus_state *s);
 int export_system(erebus_state *s, int kind, int64_t *nnz, int64_t *rows, int64_t *cols,
                   double *vals, double *rhs);
 

@@ -62,15 +62,17 @@ struct CellSort {
 };
 
 // Block-banded matrix (no pivoting LU) of one linear system.
+struct MfDevice;   // multifrontal factor storage and plan (mfront.cu)
+
 struct BandSystem {
     int64_t n = 0;             // unknowns
+    int dofs = 1;              // unknowns per P node
     int b = 0;                 // half bandwidth (max |row-col|)
     int nb = 0;                // tile size
     int NB = 0;                // tile rows/cols
     int Bb = 0;                // tile half bandwidth
-    double *tiles = nullptr;   // NB * (2Bb+1) tiles of nb*nb, column-major
-    double *invL = nullptr;    // NB inverses of the unit-lower diagonal factors
-    double *invU = nullptr;    // NB inverses of the upper diagonal factors
+    double *tiles = nullptr;   // NB * (2Bb+1) tiles of nb*nb, column-major (band LU only)
+    MfDevice *mf = nullptr;    // multifrontal LU (default direct solver)
     double *rscale = nullptr;  // row scale (1/sum|row|)
     double *rhs = nullptr;     // scaled right-hand side
     double *x = nullptr;       // solution
@@ -125,7 +127,6 @@ struct erebus_state {
 
     erebus::BandSystem hydro, thermal, gravity;
     bool sorted_valid = false;
-    bool opt_no_reuse = false;   // refactorise every solve (testing)
     double last_maxDT = 0.0;     // max|DT| of the last heat solve
 
     // phase timing with CUDA events on `stream` (enabled on request)

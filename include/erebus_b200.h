@@ -169,14 +169,21 @@ typedef struct ErebusStepStats {
     double  worst_rel_residual;/* worst final relative residual of any solve */
 } ErebusStepStats;
 
-/* Solver controls (the reference uses a direct LU, so these have no
-   counterpart; defaults come from erebus_default_solver_options). */
+/* Solver controls.  The reference solves each system with a sparse direct
+   LU (UMFPACK); here the direct solver is a no-pivot LU of the row-scaled
+   system, followed by iterative refinement to the relative residual below.
+   Defaults come from erebus_default_solver_options. */
+#define EREBUS_SOLVER_MULTIFRONTAL 0   /* nested-dissection multifrontal LU */
+#define EREBUS_SOLVER_BAND         1   /* block-banded LU in the reference's unknown order */
 typedef struct ErebusSolverOptions {
     double  hydro_rtol;        /* Stokes-Darcy relative residual target */
     double  thermal_rtol;      /* heat equation relative residual target */
     double  gravity_rtol;      /* Poisson relative residual target */
-    int32_t max_iters;         /* Krylov iteration cap per solve */
-    int32_t restart;           /* GMRES restart length */
+    int32_t max_refinements;   /* refinement corrections per solve */
+    int32_t reuse_factors;     /* 1: keep the LU factors while the scaled
+                                  matrix is bitwise unchanged */
+    int32_t direct_solver;     /* EREBUS_SOLVER_MULTIFRONTAL or EREBUS_SOLVER_BAND */
+    int32_t reserved;
 } ErebusSolverOptions;
 
 typedef struct erebus_state erebus_state;

@@ -1,0 +1,160 @@
+// CPU check of the multifrontal analysis (erebus.jl_b200/csrc/mf_plan.h).
+//
+// Test infrastructure: built by tests/test_mf_plan.py with g++ into a
+// temporary directory.  It runs the same block algorithm as the device
+// solver (tile LU without pivoting with inverted diagonal tiles, extend-add
+// of the children's Schur complements, forward and backward sweeps over the
+// fronts) in plain loops on the host, so that the analysis (tree, unknown
+// lists, extend-add maps, entry targets) is checked without a GPU.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../erebus.jl_b200/csrc/mf_plan.h"
+
+using namespace erebus;
+
+namespace {
+const int T = MF_TILE;
+
+double *tile(std::vector<double> &S, const MfFront &F, int I, int J) {
+    return &S[F.off + ((long long)J * F.Mt + I) * T * T];
+}
+// C (+)= sgn * A * B for 64 x 64 column-major tiles
+void gemm(double *C, const double *A, const double *B, double sgn) {
+    for (int c = 0; c < T; c++)
+        for (int k = 0; k < T; k++) {
+            double b = sgn * B[c * T + k];
+            for (int r = 0; r < T; r++) C[c * T + r] += A[k * T + r] * b;
+        }
+}
+bool invert(double *A) {   // Gauss-Jordan, no pivoting, in place
+    for (int k = 0; k < T; k++) {
+        double p = A[k * T + k];
+        if (!(std::fabs(p) > 0.0)) return false;
+        double ip = 1.0 / p;
+        for (int c = 0; c < T; c++)
+            if (c != k)
+                for (int r = 0; r < T; r++)
+                    if (r != k) A[c * T + r] -= A[k * T + r] * ip * A[c * T + k];
+        for (int r = 0; r < T; r++)
+            if (r != k) A[k * T + r] = -A[k * T + r] * ip;
+        for (int c = 0; c < T; c++)
+            if (c != k) A[c * T + k] *= ip;
+        A[k * T + k] = ip;
+    }
+    return true;
+}
+}  // namespace
+
+extern "C" {
+
+// Analysis statistics: fronts, levels, storage doubles, max Kt, max Mt.
+int mf_check_stats(int d, int ny, int nx, int leaf, long long *out) {
+    MfPlan P;
+    if (!mf_analyse(P, d, ny, nx, leaf)) return 1;
+    out[0] = (long long)P.fronts.size();
+    out[1] = (long long)P.level_begin.size() - 1;
+    out[2] = P.storage;
+    out[3] = P.max_kt;
+    out[4] = P.max_mt;
+    return 0;
+}
+
+// Solves the ELL system (rows x ell, rows >= n; rows >= n are ignored) for
+// right-hand side b (n values) into x.  Returns 0, or 1 analysis failed,
+// 2 entry outside the fronts, 3 zero pivot.
+int mf_check_solve(int d, int ny, int nx, int leaf, const int *cols, const double *vals,
+                   long long rows, int ell, const double *b, double *x) {
+    MfPlan P;
+    if (!mf_analyse(P, d, ny, nx, leaf)) return 1;
+    std::vector<long long> target;
+    if (!mf_targets(P, cols, rows, ell, target)) return 2;
+    std::vector<double> S(P.storage, 0.0);
+    for (long long e = 0; e < rows * ell; e++)
+        if (target[e] >= 0) S[target[e]] += vals[e];
+    for (const MfFront &F : P.fronts)
+        for (int a = F.k; a < F.Kp; a++) S[mf_elem(F, a, a)] = 1.0;
+    std::vector<double> tmp(T * T);
+    for (size_t f = 0; f < P.fronts.size(); f++) {
+        const MfFront &F = P.fronts[f];
+        for (int s = 0; s < 2; s++) {
+            int c = s == 0 ? F.c0 : F.c1;
+            if (c < 0) continue;
+            const MfFront &C = P.fronts[c];
+            const int *m = &P.eamap[F.map_off];
+            for (int bb = 0; bb < F.M; bb++) {
+                int jb = m[2 * bb + s];
+                if (jb < 0) continue;
+                for (int a = 0; a < F.M; a++) {
+                    int ia = m[2 * a + s];
+                    if (ia >= 0) S[mf_elem(F, a, bb)] += S[mf_elem(C, C.Kp + ia, C.Kp + jb)];
+                }
+            }
+        }
+        for (int K = 0; K < F.Kt; K++) {
+            if (!invert(tile(S, F, K, K))) return 3;
+            for (int I = K + 1; I < F.Mt; I++) {
+                std::fill(tmp.begin(), tmp.end(), 0.0);
+                gemm(tmp.data(), tile(S, F, I, K), tile(S, F, K, K), 1.0);
+                std::memcpy(tile(S, F, I, K), tmp.data(), sizeof(double) * T * T);
+            }
+            for (int J = K + 1; J < F.Mt; J++)
+                for (int I = K + 1; I < F.Mt; I++)
+                    if (I < F.Kt || J < F.Kt)
+                        gemm(tile(S, F, I, J), tile(S, F, I, K), tile(S, F, K, J), -1.0);
+        }
+        for (int J = F.Kt; J < F.Mt; J++)
+            for (int I = F.Kt; I < F.Mt; I++)
+                for (int K = 0; K < F.Kt; K++)
+                    gemm(tile(S, F, I, J), tile(S, F, I, K), tile(S, F, K, J), -1.0);
+    }
+    // forward sweep
+    std::vector<double> w(b, b + P.n), fv(P.vec, 0.0);
+    for (size_t f = 0; f < P.fronts.size(); f++) {
+        const MfFront &F = P.fronts[f];
+        double *v = &fv[F.vec_off];
+        const int *var = &P.vars[F.var_off];
+        const int *m = &P.eamap[F.map_off];
+        for (int a = 0; a < F.M; a++) {
+            double s = (a < F.Kp && var[a] >= 0) ? w[var[a]] : 0.0;
+            for (int q = 0; q < 2; q++) {
+                int c = q == 0 ? F.c0 : F.c1;
+                if (c >= 0 && m[2 * a + q] >= 0) s += fv[P.fronts[c].vec_off + P.fronts[c].Kp + m[2 * a + q]];
+            }
+            v[a] = s;
+        }
+        for (int K = 0; K < F.Kt; K++)
+            for (int I = K + 1; I < F.Mt; I++) {
+                const double *L = tile(S, F, I, K);
+                for (int c = 0; c < T; c++)
+                    for (int r = 0; r < T; r++) v[I * T + r] -= L[c * T + r] * v[K * T + c];
+            }
+    }
+    // backward sweep
+    for (size_t f = P.fronts.size(); f-- > 0;) {
+        const MfFront &F = P.fronts[f];
+        double *v = &fv[F.vec_off];
+        const int *var = &P.vars[F.var_off];
+        for (int a = F.Kp; a < F.M; a++) v[a] = var[a] >= 0 ? w[var[a]] : 0.0;
+        for (int K = F.Kt - 1; K >= 0; K--) {
+            double t[T];
+            for (int r = 0; r < T; r++) t[r] = v[K * T + r];
+            for (int J = K + 1; J < F.Mt; J++) {
+                const double *U = tile(S, F, K, J);
+                for (int c = 0; c < T; c++)
+                    for (int r = 0; r < T; r++) t[r] -= U[c * T + r] * v[J * T + c];
+            }
+            const double *Di = tile(S, F, K, K);
+            for (int r = 0; r < T; r++) {
+                double s = 0.0;
+                for (int c = 0; c < T; c++) s += Di[c * T + r] * t[c];
+                v[K * T + r] = s;
+            }
+        }
+        for (int a = 0; a < F.k; a++) w[var[a]] = v[a];
+    }
+    std::memcpy(x, w.data(), sizeof(double) * P.n);
+    return 0;
+}
+}
