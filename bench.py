@@ -1,7 +1,7 @@
 """Benchmark: MIC timesteps per second of the plain FP64 GPU path.
 
-Workload: the synthetic 141x141 planetesimal (490,000 markers, 5x5 per
-cell; 140 km box, 50 km rock body in sticky air; per-marker porosity
+Workload (default): the synthetic 141x141 planetesimal (490,000 markers, 5x5
+per cell; 140 km box, 50 km rock body in sticky air; per-marker porosity
 U(0.05, 0.25) and log-uniform rock viscosity 1e18-1e20 Pa s).  A step is one
 whole timestep of simulation_loop (src/Erebus.jl:6370-7235).  With N GPUs
 (torchrun) every rank advances its own planetesimal (replicas; the path has
@@ -9,6 +9,7 @@ no exchange step) and `value` is all ranks' timesteps over the slowest
 rank's device time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload planetesimal_401] [--direct-solver band]
 """
 import argparse
 import json
@@ -61,8 +62,8 @@ def config_dict(pkg, name, extra=None):
     c = pkg.CONFIGS[name]
     d = {"workload": name, "grid": "%dx%d basic nodes" % (c["N"], c["N"]),
          "markers_per_cell": "%dx%d" % (c["mpc"], c["mpc"]),
-         "l2": "inputs larger than L2 (band LU storage ~1.9 GB, 490k-marker SoA ~110 MB "
-               "streamed every step)"}
+         "l2": "inputs larger than L2: the Stokes-Darcy factor storage (1.6 GB at 141x141) "
+               "is written and read every timestep, and the marker arrays are streamed"}
     if extra:
         d.update(extra)
     return d
@@ -78,7 +79,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), "--query-gpu=" + q,
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -109,6 +110,28 @@ class Clocks:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_peak():
+    """Measured FP64 dense throughput of this GPU: cuBLAS DGEMM (torch.matmul,
+    8192^3), best of 3, TFLOP/s."""
+    import torch
+    n = 8192
+    a = torch.rand(n, n, dtype=torch.float64, device="cuda")
+    b = torch.rand(n, n, dtype=torch.float64, device="cuda")
+    a @ b
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1000.0) / 1e12
 
 
 def dist_setup(n):
@@ -174,42 +197,43 @@ def run_reference(args):
         return 0
     pkg = load_pkg()
     O = load_oracle()
-    st = pkg.make_state(WORKLOAD)
+    st = pkg.make_state(args.workload)
     o = O.Oracle(st)
-    for ts in range(1, args.warmup + 1):
+    # each step is a bounded sample of the workload: the oracle needs about
+    # 10 s per 141x141 timestep on 16 cores, so the reference arm runs at
+    # most 2 timed steps after 1 untimed one
+    warm = min(args.warmup, 1)
+    steps = min(args.steps, 2)
+    for ts in range(1, warm + 1):
         o.step(ts)
     t0 = time.perf_counter()
-    for ts in range(args.warmup + 1, args.warmup + args.steps + 1):
+    for ts in range(warm + 1, warm + steps + 1):
         o.step(ts)
     el = time.perf_counter() - t0
-    v = args.steps / el
+    v = steps / el
     cores = os.cpu_count()
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000 * el / args.steps, "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+            "ms_per_step": 1000 * el / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict(pkg, WORKLOAD),
+            "config": config_dict(pkg, args.workload),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "timesteps %d-%d after %d untimed, oracle restatement "
-                                       "of the reference (Julia is not available) with "
-                                       "SuperLU solves" % (args.warmup + 1,
-                                                           args.warmup + args.steps,
-                                                           args.warmup)},
+                             "sample": "timesteps %d-%d after %d untimed (requested %d "
+                                       "timed, %d warm-up), oracle restatement of the "
+                                       "reference (Julia is not available) with SuperLU "
+                                       "solves, OpenMP on the marker loops the reference "
+                                       "threads" % (warm + 1, warm + steps, warm, args.steps,
+                                                    args.warmup)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def algorithmic_bytes(sim, st):
-    """Bytes each phase must move once (per launch of the phase)."""
+def algorithmic_bytes(st):
+    """Bytes each marker phase must move once (per launch of the phase)."""
     g = st.g
     n = st.marknum
     nodes = g.Nx1 * g.Ny1
-    tiles = lambda sysn: sysn  # placeholder for clarity
-    nbt = 64
-    NBh = (6 * nodes + nbt - 1) // nbt
-    Bbh = (6 * g.Ny1 + 2 + nbt - 1) // nbt
-    band_h = NBh * (2 * Bbh + 1) * nbt * nbt * 8
     return {
         # read 16 marker fields (129 B) + write 7 derived (56 B); ~217 B per
         # P node of normalised outputs
@@ -217,9 +241,6 @@ def algorithmic_bytes(sim, st):
         "rk4": 97 * n,
         "nodes_to_markers": 137 * n,
         "reaction": 73 * n,
-        # the band is read and written once by the factorisation
-        "hydro_factor": 2 * band_h,
-        "hydro_solve": band_h,
     }
 
 
@@ -227,8 +248,10 @@ def run_ours(args):
     rank, world, local = dist_setup(args.gpus)
     import torch
     pkg = load_pkg()
-    st = pkg.make_state(WORKLOAD)
+    solver = {"multifrontal": 0, "band": 1}[args.direct_solver]
+    st = pkg.make_state(args.workload)
     sim = pkg.Simulation(st)
+    sim.set_solver_options(direct_solver=solver)
     for ts in range(1, args.warmup + 1):
         sim.step(ts)
     sim.enable_phase_timing(True)
@@ -250,13 +273,15 @@ def run_ours(args):
     ms_max = max_over_ranks(ms, world)
     launches = sim.kernel_launches() - l0
     phases = sim.phase_times()
+    fstats = {k: sim.factor_stats(i) for i, k in enumerate(("hydro", "thermal", "gravity"))}
     value = world * args.steps / (ms_max / 1000.0)
 
     # end to end through the public API: host buffers (pinned) uploaded,
     # one timestep, results downloaded, every step
-    st2 = pin_host_state(pkg.make_state(WORKLOAD))
+    st2 = pin_host_state(pkg.make_state(args.workload))
     sim.close()
     sim2 = pkg.Simulation(st2)
+    sim2.set_solver_options(direct_solver=solver)
     for ts in range(1, 3):
         sim2.step(ts)
     sim2.download()
@@ -267,7 +292,7 @@ def run_ours(args):
     d2h = h2d
     stream2 = torch.cuda.ExternalStream(sim2.stream_handle())
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ne2e = max(2, min(args.steps, 3))
+    ne2e = max(3, min(args.steps, 10))
     barrier(world)
     torch.cuda.synchronize()
     e2.record(stream2)
@@ -285,7 +310,8 @@ def run_ours(args):
 
     if rank == 0:
         hbm, src = peaks()
-        ab = algorithmic_bytes(None, st)
+        f64 = fp64_peak()
+        ab = algorithmic_bytes(st)
         per = {}
         for k, (t, c) in phases.items():
             if c:
@@ -294,25 +320,44 @@ def run_ours(args):
                     ent["GBps"] = ab[k] / (t / c / 1000.0) / 1e9
                 per[k] = ent
         dom = max(per, key=lambda k: per[k]["ms_total"])
-        roof = None
-        hbm_dom = dom if dom in ab else max((k for k in per if k in ab),
-                                            key=lambda k: per[k]["ms_total"])
-        a = per[hbm_dom]["GBps"]
-        roof = {"bound": "hbm", "kernel": hbm_dom, "achieved": a, "peak": hbm, "unit": "GB/s",
-                "frac": a / hbm, "peak_source": src, "traffic": None,
-                "bytes_per_launch": ab[hbm_dom],
-                "note": "dominant phase by device time: %s" % dom}
-        cpu = None if args.no_cpu_baseline else cpu_baseline(pkg, load_oracle(), WORKLOAD)
+        fh = fstats["hydro"]
+        kname = "k_mf_factor" if solver == 0 else "k_band_factor"
+        tf = fh.flops / (per["hydro_factor"]["ms_per_launch"] / 1000.0) / 1e12
+        roof = {"bound": "fp64", "kernel": kname, "phase": "hydro_factor",
+                "achieved": tf, "peak": f64, "unit": "TFLOP/s", "frac": tf / f64,
+                "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.matmul)",
+                "traffic": None,
+                "flops_per_launch": fh.flops,
+                "note": "dominant phase by device time: %s; FP64 flops of the 64x64 tile "
+                        "algorithm (padding included); DRAM traffic per launch is in the "
+                        "committed ncu summary" % dom}
+        solve_ms = per["hydro_solve"]["ms_per_launch"] / max(
+            1.0, sum(s.hydro_solves for s in stats) / max(1, sum(s.titer for s in stats)))
+        roof_solve = {"bound": "hbm", "kernel": "k_mf_solve" if solver == 0 else "k_band_solve",
+                      "achieved": fh.solve_bytes / (solve_ms / 1000.0) / 1e9, "peak": hbm,
+                      "unit": "GB/s", "peak_source": src,
+                      "frac": fh.solve_bytes / (solve_ms / 1000.0) / 1e9 / hbm,
+                      "bytes_per_launch": fh.solve_bytes,
+                      "note": "factor bytes read per forward+backward solve over the "
+                              "hydro_solve phase time per refinement solve"}
+        cpu = None
+        if not args.no_cpu_baseline and args.workload == WORKLOAD:
+            cpu = cpu_baseline(pkg, load_oracle(), args.workload)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": config_dict(pkg, WORKLOAD,
+                "config": config_dict(pkg, args.workload,
                                       {"parallelism": "replicas x%d" % world,
+                                       "direct_solver": args.direct_solver,
                                        "titer_per_step": [s.titer for s in stats],
-                                       "factorizations": [s.factorizations for s in stats]}),
-                "roofline": roof, "phases": per, "cpu_baseline": cpu, "clocks": ck,
-                "e2e": e2e, "gpu_launches": launches}
+                                       "hydro_solves": sum(s.hydro_solves for s in stats),
+                                       "thermal_solves": sum(s.thermal_solves for s in stats),
+                                       "gravity_solves": sum(s.gravity_solves for s in stats),
+                                       "factor_storage_GB": {k: v.storage_bytes / 1e9
+                                                             for k, v in fstats.items()}}),
+                "roofline": roof, "roofline_solve": roof_solve, "phases": per,
+                "cpu_baseline": cpu, "clocks": ck, "e2e": e2e, "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -323,10 +368,13 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=["planetesimal_41", "planetesimal_141", "planetesimal_401"])
+    ap.add_argument("--direct-solver", default="multifrontal", choices=["multifrontal", "band"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

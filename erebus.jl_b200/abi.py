@@ -145,10 +145,18 @@ class ErebusSolveStats(Structure):
 
 class ErebusStepStats(Structure):
     _fields_ = [
-        ("titer", c_int32), ("iplast_total", c_int32), ("krylov_total", c_int32),
-        ("thermal_total", c_int32), ("gravity_iters", c_int32), ("factorizations", c_int32),
+        ("titer", c_int32), ("iplast_total", c_int32), ("hydro_solves", c_int32),
+        ("thermal_solves", c_int32), ("gravity_solves", c_int32), ("factorizations", c_int32),
         ("marknum", c_int64), ("dt", c_double), ("timesum", c_double),
         ("maxT", c_double), ("worst_rel_residual", c_double),
+    ]
+
+
+class ErebusFactorStats(Structure):
+    _fields_ = [
+        ("direct_solver", c_int32), ("fronts", c_int32), ("levels", c_int32),
+        ("factorizations", c_int32), ("unknowns", c_int64), ("storage_bytes", c_int64),
+        ("flops", c_double), ("solve_bytes", c_double),
     ]
 
 

@@ -316,6 +316,18 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
     return EREBUS_OK;
 }
 
+int erebus_factor_stats(erebus_state *s, int32_t system, ErebusFactorStats *out) {
+    if (!s || !out || system < 0 || system > 2) return EREBUS_EINVAL;
+    BandSystem &sys = band_of(s, system);
+    std::memset(out, 0, sizeof(*out));
+    out->direct_solver = s->opt.direct_solver;
+    if (use_multifrontal(s)) mf_stats(s, sys, out);
+    else band_stats(sys, out);
+    out->unknowns = sys.n;
+    out->factorizations = sys.factorizations;
+    return EREBUS_OK;
+}
+
 int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o) {
     if (!s || !o) return EREBUS_EINVAL;
     if (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL && o->direct_solver != EREBUS_SOLVER_BAND)
@@ -601,7 +613,7 @@ int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st) {
     timer_begin(s, PH_GRAVITY);
     TRY(erebus_gravity(s, &gs));
     timer_end(s, PH_GRAVITY);
-    stats.gravity_iters = gs.iterations;
+    stats.gravity_solves = gs.iterations;
     worst = gs.rel_residual;
     double dt = std::fmin(s->dt * p.dtcoefup, p.dt_longest);   // E:6619
     size_t npb = (size_t)s->g.Nx1 * s->g.Ny1 * 8, nbb = (size_t)s->g.Nx * s->g.Ny;
@@ -623,14 +635,14 @@ int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st) {
             int conv = 0;
             ErebusSolveStats hs = {};
             TRY(erebus_hydromech_pass(s, &dt, iplast, &conv, &hs));
-            stats.krylov_total += hs.iterations;
+            stats.hydro_solves += hs.iterations;
             worst = std::fmax(worst, hs.rel_residual);
             if (conv) break;
         }
         ErebusSolveStats ts = {};
         double maxDT = 0.0;
         TRY(erebus_thermal_solve(s, dt, timestep, &maxDT, &ts));
-        stats.thermal_total += ts.iterations;
+        stats.thermal_solves += ts.iterations;
         worst = std::fmax(worst, ts.rel_residual);
         if (titer == 1 && maxDT > p.DTmax) dt *= p.DTmax * (1.0 / maxDT);   // E:4187-4197
         double pferr = slot(s, X_PFERR), dmpmax = slot(s, X_DMP);        // E:4216-4223

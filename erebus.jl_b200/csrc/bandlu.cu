@@ -567,6 +567,19 @@ static int lu_error(erebus_state *s, BandSystem &sys, const char *what) {
     return EREBUS_OK;
 }
 
+void band_stats(const BandSystem &sys, ErebusFactorStats *o) {
+    double tiles = 0.0;
+    for (int K = 0; K < sys.NB; K++) {
+        int nJ = std::min(sys.Bb, sys.NB - 1 - K);
+        tiles += 1 + nJ + (double)nJ * nJ;
+    }
+    o->fronts = 0;
+    o->levels = sys.NB;
+    o->storage_bytes = (int64_t)tiles_bytes(sys);
+    o->flops = tiles * 2.0 * NB_TILE * NB_TILE * NB_TILE;
+    o->solve_bytes = (double)tiles_bytes(sys);
+}
+
 bool use_multifrontal(const erebus_state *s) {
     return s->opt.direct_solver != EREBUS_SOLVER_BAND;
 }

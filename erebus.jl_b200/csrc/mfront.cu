@@ -522,6 +522,10 @@ static cudaError_t upload(T **dst, const std::vector<T> &src, cudaStream_t st) {
     return e;
 }
 
+// Leaves of 16 nodes for the 6-unknown system (96 unknowns), 64 nodes for
+// the scalar ones, so that a leaf fills its 64-wide tiles.
+static int mf_leaf(int dofs) { return dofs >= 4 ? 16 : 64; }
+
 // Builds the plan of `sys` from the column pattern of its assembled ELL
 // matrix (on the device) and uploads it.
 static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
@@ -535,10 +539,7 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
     if (!rc) rc = check_cuda(s, cudaStreamSynchronize(s->stream), "mf pattern");
     if (rc) return rc;
     MfPlan &P = D->plan;
-    // leaves of 16 nodes for the 6-unknown system (96 unknowns), 64 nodes
-    // for the scalar ones, so a leaf fills its 64-wide tiles
-    const int leaf = dofs >= 4 ? 16 : 64;
-    if (!mf_analyse(P, dofs, s->g.Ny1, s->g.Nx1, leaf) || P.n != sys.n) {
+    if (!mf_analyse(P, dofs, s->g.Ny1, s->g.Nx1, mf_leaf(dofs)) || P.n != sys.n) {
         s->last_error = "multifrontal analysis failed";
         return EREBUS_EINVAL;
     }
@@ -613,6 +614,26 @@ int mf_factor(erebus_state *s, BandSystem &sys) {
     sys.factored = true;
     sys.factorizations++;
     return EREBUS_OK;
+}
+
+void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o) {
+    MfPlan P;
+    mf_analyse(P, sys.dofs, s->g.Ny1, s->g.Nx1, mf_leaf(sys.dofs));
+    double tiles = 0.0, rd = 0.0;
+    for (const MfFront &F : P.fronts) {
+        tiles += F.Kt;   // inverses
+        for (int K = 0; K < F.Kt; K++) {
+            int R = F.Mt - K - 1, e = F.Kt - K - 1;
+            tiles += R + e * R + (F.Mt - F.Kt) * e;
+        }
+        tiles += (double)(F.Mt - F.Kt) * (F.Mt - F.Kt) * F.Kt;
+        rd += 2.0 * F.Kt * F.Mt - (double)F.Kt * F.Kt;
+    }
+    o->fronts = (int32_t)P.fronts.size();
+    o->levels = (int32_t)P.level_begin.size() - 1;
+    o->storage_bytes = P.storage * (int64_t)sizeof(double);
+    o->flops = tiles * 2.0 * T2 * NB_TILE;
+    o->solve_bytes = rd * T2 * sizeof(double);
 }
 
 int mf_solve(erebus_state *s, BandSystem &sys, double *w) {

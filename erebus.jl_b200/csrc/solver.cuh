@@ -57,6 +57,8 @@ int assemble_system(erebus_state *s, int kind);
 int mf_factor(erebus_state *s, BandSystem &sys);
 int mf_solve(erebus_state *s, BandSystem &sys, double *w);
 void mf_release(BandSystem &sys);
+void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o);
+void band_stats(const BandSystem &sys, ErebusFactorStats *o);
 // true when `sys` is factored by the multifrontal LU (else the band LU)
 bool use_multifrontal(const erebus_state *s);
 int export_system(erebus_state *s, int kind, int64_t *nnz, int64_t *rows, int64_t *cols,

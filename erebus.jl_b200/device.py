@@ -11,8 +11,8 @@ import os
 
 import numpy as np
 
-from .abi import (STATUS_NAMES, ErebusGridHost, ErebusMarkersHost, ErebusParams,
-                  ErebusSolverOptions, ErebusSolveStats, ErebusStepStats,
+from .abi import (STATUS_NAMES, ErebusFactorStats, ErebusGridHost, ErebusMarkersHost,
+                  ErebusParams, ErebusSolverOptions, ErebusSolveStats, ErebusStepStats,
                   ErebusSumsHost)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -26,7 +26,7 @@ EXPORTS = [
     "erebus_markers_to_nodes", "erebus_gravity", "erebus_thermochemical_reaction",
     "erebus_hydromech_pass", "erebus_thermal_solve", "erebus_nodes_to_markers",
     "erebus_advect_rk4", "erebus_replenish", "erebus_step", "erebus_export_hydromech",
-    "erebus_apply_hydromech", "erebus_kernel_launches",
+    "erebus_apply_hydromech", "erebus_kernel_launches", "erebus_factor_stats",
 ]
 
 
@@ -60,6 +60,7 @@ def load_library(path=LIB_PATH):
         "erebus_create": [ctypes.POINTER(ErebusParams), I64, PP],
         "erebus_destroy": [P],
         "erebus_set_solver_options": [P, ctypes.POINTER(ErebusSolverOptions)],
+        "erebus_factor_stats": [P, I32, ctypes.POINTER(ErebusFactorStats)],
         "erebus_upload_markers": [P, ctypes.POINTER(ErebusMarkersHost), I64],
         "erebus_download_markers": [P, ctypes.POINTER(ErebusMarkersHost), pI64],
         "erebus_upload_grid": [P, ctypes.POINTER(ErebusGridHost)],
@@ -241,6 +242,13 @@ class Simulation:
             self.h, dt, ctypes.byref(nnz), rows.ctypes.data, cols.ctypes.data,
             vals.ctypes.data, R.ctypes.data))
         return rows, cols, vals, R
+
+    def factor_stats(self, system):
+        """ErebusFactorStats of system 0 (Stokes-Darcy), 1 (heat) or 2 (gravity)."""
+        o = ErebusFactorStats()
+        self._check("erebus_factor_stats",
+                    self.L.erebus_factor_stats(self.h, system, ctypes.byref(o)))
+        return o
 
     def kernel_launches(self):
         n = ctypes.c_int64()

@@ -158,9 +158,9 @@ typedef struct ErebusSolveStats {
 typedef struct ErebusStepStats {
     int32_t titer;             /* thermochemical iterations taken */
     int32_t iplast_total;      /* plastic iterations summed over titer */
-    int32_t krylov_total;      /* Stokes-Darcy Krylov iterations summed */
-    int32_t thermal_total;     /* heat-equation Krylov iterations summed */
-    int32_t gravity_iters;     /* gravity refinement iterations */
+    int32_t hydro_solves;      /* Stokes-Darcy triangular solves (refinement steps) summed */
+    int32_t thermal_solves;    /* heat-equation triangular solves summed */
+    int32_t gravity_solves;    /* gravity triangular solves */
     int32_t factorizations;    /* LU factorisations (1000 * Stokes-Darcy + heat) */
     int64_t marknum;           /* markers in use after replenishment */
     double  dt;                /* timestep taken [s] */
@@ -186,6 +186,24 @@ typedef struct ErebusSolverOptions {
     int32_t reserved;
 } ErebusSolverOptions;
 
+/* Size and work of one system's direct solver (diagnostics; no reference
+   counterpart).  flops counts the FP64 multiply-adds of the 64 x 64 tile
+   algorithm (2 flops each, padding included); solve_bytes is the factor
+   storage one forward plus backward solve reads. */
+#define EREBUS_SYSTEM_HYDRO   0
+#define EREBUS_SYSTEM_THERMAL 1
+#define EREBUS_SYSTEM_GRAVITY 2
+typedef struct ErebusFactorStats {
+    int32_t direct_solver;     /* EREBUS_SOLVER_* in use */
+    int32_t fronts;            /* multifrontal fronts (0 for the band LU) */
+    int32_t levels;            /* tree levels (band LU: tile rows) */
+    int32_t factorizations;    /* factorisations so far */
+    int64_t unknowns;
+    int64_t storage_bytes;     /* factor storage */
+    double  flops;             /* per factorisation */
+    double  solve_bytes;       /* per solve */
+} ErebusFactorStats;
+
 typedef struct erebus_state erebus_state;
 
 /* ---- parameters --------------------------------------------------------- */
@@ -201,6 +219,8 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity,
                   erebus_state **out);
 int erebus_destroy(erebus_state *s);
 int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o);
+/* Sizes and work of the direct solver of `system` (EREBUS_SYSTEM_*). */
+int erebus_factor_stats(erebus_state *s, int32_t system, ErebusFactorStats *out);
 /* Last CUDA/solver error text for a state (NUL-terminated, owned by state). */
 const char *erebus_last_error(const erebus_state *s);
 
