@@ -14,7 +14,8 @@
 //              diagonal tile D_K (Gauss-Jordan), L_IK = A_IK D_K^{-1}, and
 //              the rank-64 update of the eliminated rows and columns; last
 //              the Schur complement of the update block with inner dimension
-//              Kp (tile GEMMs, FP64 FMA);
+//              Kp (tile products on the FP64 tensor cores, operands streamed
+//              through a cp.async pipeline);
 //   solve      (k_mf_solve) forward over the levels from the leaves, backward
 //              from the root; each front gathers its children's update
 //              vectors and its ring solution through index maps.
@@ -94,14 +95,8 @@ __global__ void k_mf_pad(MfView V, int nfronts) {
 }
 
 // ---------------------------------------------------------------------------
-// factor: CTA-wide tile operations (FactorSmem staging, 256 threads)
+// factor: CTA-wide tile operations (256 threads)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void negate(double a[4][4]) {
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) a[i][j] = -a[i][j];
-}
 
 // Tile (I, J) of front f += the children's Schur complement entries that
 // map onto it (child 0 first, then child 1).
@@ -129,55 +124,55 @@ __device__ void mf_extend_add_tile(const MfView &V, const MfFront &f, int I, int
     }
 }
 
-__device__ void mf_invert_tile(double *T, FactorSmem &S, int *err) {
+// Inverts tile T in place (Gauss-Jordan in the FFMA register layout).
+__device__ void mf_invert_tile(double *T, MmaSmem &S, int *err) {
     double a[4][4];
-    stage_tile(S.Cs, T);
+    double *P = S.stage[0];
+    stage_tile(P, T);
     __syncthreads();
-    regs_from_smem(S.Cs, a);
+    regs_from_smem(P, a);
     __syncthreads();
     tile_inverse(a, S.vec, err);
-    regs_to_smem(S.Cs, a);
+    regs_to_smem(P, a);
     __syncthreads();
-    unstage_tile(T, S.Cs);
+    unstage_tile(T, P);
     __syncthreads();
 }
 
 // L_IK = A_IK D_K^{-1} (tile (K,K) holds D_K^{-1})
-__device__ void mf_l_tile(const MfView &V, const MfFront &f, int I, int K, FactorSmem &S) {
-    double acc[4][4] = {};
-    double *T = ftile(V, f, I, K);
-    stage_tile(S.As, T);
-    stage_tile_t(S.Bt, ftile(V, f, K, K));
-    __syncthreads();
-    gemm_acc(S.As, S.Bt, acc);
-    regs_to_smem(S.Cs, acc);
-    __syncthreads();
-    unstage_tile(T, S.Cs);
+__device__ void mf_l_tile(const MfView &V, const MfFront &f, int I, int K, MmaSmem &S) {
+    MmaAcc acc;
+    frag_zero(acc);
+    const double *A = ftile(V, f, I, K), *B = ftile(V, f, K, K);
+    mma_tiles(
+        S, 1, [&](int) { return A; }, [&](int) { return B; }, acc);
+    frag_store(ftile(V, f, I, K), acc, 1.0);
     __syncthreads();
 }
 
 // A_IJ -= sum_{K in [k0, k1)} L_IK A_KJ; optionally invert the result.
 __device__ void mf_update_tile(const MfView &V, const MfFront &f, int I, int J, int k0,
-                               int k1, FactorSmem &S, int *err, bool invert) {
-    double acc[4][4];
+                               int k1, MmaSmem &S, int *err, bool invert) {
+    MmaAcc acc;
     double *C = ftile(V, f, I, J);
-    stage_tile(S.Cs, C);
-    __syncthreads();
-    regs_from_smem(S.Cs, acc);
-    negate(acc);
-    for (int K = k0; K < k1; K++) {
+    frag_load(C, acc, -1.0);
+    mma_tiles(
+        S, k1 - k0, [&](int p) { return (const double *)ftile(V, f, I, k0 + p); },
+        [&](int p) { return (const double *)ftile(V, f, k0 + p, J); }, acc);
+    if (invert) {
+        double a[4][4];
+        double *P = S.stage[0];
+        frag_to_smem(P, acc, -1.0);
         __syncthreads();
-        stage_tile(S.As, ftile(V, f, I, K));
-        stage_tile_t(S.Bt, ftile(V, f, K, J));
+        regs_from_smem(P, a);
         __syncthreads();
-        gemm_acc(S.As, S.Bt, acc);
+        tile_inverse(a, S.vec, err);
+        regs_to_smem(P, a);
+        __syncthreads();
+        unstage_tile(C, P);
+    } else {
+        frag_store(C, acc, -1.0);
     }
-    negate(acc);
-    __syncthreads();
-    if (invert) tile_inverse(acc, S.vec, err);
-    regs_to_smem(S.Cs, acc);
-    __syncthreads();
-    unstage_tile(C, S.Cs);
     __syncthreads();
 }
 
@@ -202,7 +197,7 @@ __device__ __forceinline__ void mf_upd_ij(const MfFront &f, int K, int u, int &I
 }
 
 // The whole partial LU of one front by one CTA.
-__device__ void mf_factor_local(const MfView &V, const MfFront &f, FactorSmem &S, int *err) {
+__device__ void mf_factor_local(const MfView &V, const MfFront &f, MmaSmem &S, int *err) {
     if (f.c0 >= 0 || f.c1 >= 0) {
         for (int t = 0; t < f.Mt * f.Mt; t++) mf_extend_add_tile(V, f, t % f.Mt, t / f.Mt);
         __threadfence_block();
@@ -241,7 +236,7 @@ __device__ void mf_for_tasks(const MfView &V, int fb, int fe, Count count, Task 
 __global__ void __launch_bounds__(LU_THREADS, 2)
 k_mf_factor(MfView V, unsigned int *bar, int *err) {
     extern __shared__ __align__(16) double smem_raw[];
-    FactorSmem &S = *reinterpret_cast<FactorSmem *>(smem_raw);
+    MmaSmem &S = *reinterpret_cast<MmaSmem *>(smem_raw);
     const int G = gridDim.x;
     for (int p = 0; p < V.nlev; p++) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
@@ -595,7 +590,7 @@ int mf_factor(erebus_state *s, BandSystem &sys) {
                   sys.err);
     int nf = (int)D.plan.fronts.size();
     EREBUS_LAUNCH(s, k_mf_pad, nf, 64, 0, V, nf);
-    size_t smem = sizeof(FactorSmem);
+    size_t smem = sizeof(MmaSmem);
     cudaFuncSetAttribute(k_mf_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int blocks = mf_blocks(s, (const void *)k_mf_factor, smem);
     if (blocks < 1) {

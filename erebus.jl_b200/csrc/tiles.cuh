@@ -179,4 +179,168 @@ struct FactorSmem {
     double vec[2 * 2 * NB_TILE];
 };
 
+// ---------------------------------------------------------------------------
+// FP64 tensor-core tile products (mma.sync m16n8k16 .f64)
+//
+// A 64 x 64 result tile is held in registers by the 8 warps of the CTA:
+// warp w owns rows 32 (w & 1) .. +32 and columns 16 (w >> 1) .. +16 as
+// 2 x 2 fragments of 16 x 8; fragment element q of thread (g = lane / 4,
+// t = lane % 4) is row g + 8 (q / 2), column 2 t + q % 2.  Operand tiles
+// stream through shared memory in K-chunks of 32 with cp.async (16-byte
+// copies that bypass L1, so data other CTAs wrote is read from L2), three
+// stages deep: A chunks column-major with leading dimension 68, B chunks
+// column-major with leading dimension 36, both chosen so that the fragment
+// loads of a warp hit every bank pair exactly twice.
+// ---------------------------------------------------------------------------
+constexpr int MMA_LA = 68, MMA_LB = 36, MMA_KC = 32, MMA_NSTAGE = 3;
+constexpr int MMA_STAGE = MMA_KC * MMA_LA + NB_TILE * MMA_LB;   // doubles per stage
+
+struct MmaSmem {
+    double stage[MMA_NSTAGE][MMA_STAGE];
+    double vec[2 * 2 * NB_TILE];
+};
+static_assert(MMA_STAGE >= STILE, "a stage holds a padded tile");
+
+typedef double MmaAcc[2][2][4];
+
+static __device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+static __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
+                 : "memory");
+}
+static __device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+static __device__ __forceinline__ void cp_async_wait1() {
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+static __device__ __forceinline__ void cp_async_wait0() {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// Copies K-chunk h (columns 32 h .. 32 h + 31 of A, rows of B) of the
+// column-major 64 x 64 tiles A and B into stage `st`.
+static __device__ __forceinline__ void mma_load_chunk(double *st, const double *A, const double *B,
+                                                      int h) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int e = threadIdx.x + 256 * q;
+        int col = e >> 5, rp = (e & 31) * 2;
+        cp_async16(st + col * MMA_LA + rp, A + (h * MMA_KC + col) * NB_TILE + rp);
+    }
+    double *sb = st + MMA_KC * MMA_LA;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int e = threadIdx.x + 256 * q;
+        int c = e >> 4, kp = (e & 15) * 2;
+        cp_async16(sb + c * MMA_LB + kp, B + c * NB_TILE + h * MMA_KC + kp);
+    }
+}
+
+static __device__ __forceinline__ void mma_16816(double c[4], const double a[8], const double b[4]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+        "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]),
+          "d"(a[7]), "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+// acc += (chunk's A part) * (chunk's B part)
+static __device__ __forceinline__ void mma_chunk(const double *st, MmaAcc acc) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int rb = (w & 1) * 32, cb = (w >> 1) * 16;
+    const double *sa = st, *sb = st + MMA_KC * MMA_LA;
+#pragma unroll
+    for (int ks = 0; ks < MMA_KC; ks += 16) {
+        double a[2][8], b[2][4];
+#pragma unroll
+        for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                a[mi][i] = sa[(ks + t + 4 * (i >> 1)) * MMA_LA + rb + mi * 16 + g + 8 * (i & 1)];
+#pragma unroll
+        for (int ni = 0; ni < 2; ni++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) b[ni][i] = sb[(cb + ni * 8 + g) * MMA_LB + ks + t + 4 * i];
+#pragma unroll
+        for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+            for (int ni = 0; ni < 2; ni++) mma_16816(acc[mi][ni], a[mi], b[ni]);
+    }
+}
+
+// acc += sum_{p < np} tileA(p) * tileB(p) (global column-major tiles),
+// three-stage cp.async pipeline.  Ends with the stages free.
+template <class TA, class TB>
+static __device__ void mma_tiles(MmaSmem &S, int np, TA tileA, TB tileB, MmaAcc acc) {
+    const int nq = 2 * np;
+#pragma unroll 1
+    for (int q = 0; q < 2; q++) {
+        if (q < nq) mma_load_chunk(S.stage[q], tileA(q >> 1), tileB(q >> 1), q & 1);
+        cp_async_commit();
+    }
+#pragma unroll 1
+    for (int q = 0; q < nq; q++) {
+        cp_async_wait1();
+        __syncthreads();
+        if (q + 2 < nq)
+            mma_load_chunk(S.stage[(q + 2) % MMA_NSTAGE], tileA((q + 2) >> 1), tileB((q + 2) >> 1),
+                           (q + 2) & 1);
+        cp_async_commit();
+        mma_chunk(S.stage[q % MMA_NSTAGE], acc);
+    }
+    cp_async_wait0();
+    __syncthreads();
+}
+
+// fragment element (mi, ni, q) -> (row, column) of the tile
+static __device__ __forceinline__ int frag_row(int mi, int q) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    return (w & 1) * 32 + mi * 16 + (lane >> 2) + 8 * (q >> 1);
+}
+static __device__ __forceinline__ int frag_col(int ni, int q) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    return (w >> 1) * 16 + ni * 8 + 2 * (lane & 3) + (q & 1);
+}
+static __device__ __forceinline__ void frag_zero(MmaAcc acc) {
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 2; ni++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[mi][ni][q] = 0.0;
+}
+// acc = sign * C (global column-major tile, read through L2)
+static __device__ __forceinline__ void frag_load(const double *C, MmaAcc acc, double sign) {
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 2; ni++)
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                acc[mi][ni][q] = sign * __ldcg(&C[frag_col(ni, q) * NB_TILE + frag_row(mi, q)]);
+}
+static __device__ __forceinline__ void frag_store(double *C, const MmaAcc acc, double sign) {
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 2; ni++)
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                C[frag_col(ni, q) * NB_TILE + frag_row(mi, q)] = sign * acc[mi][ni][q];
+}
+// fragments -> shared-memory tile (column-major, ld LDS)
+static __device__ __forceinline__ void frag_to_smem(double *T, const MmaAcc acc, double sign) {
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 2; ni++)
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                T[frag_col(ni, q) * LDS + frag_row(mi, q)] = sign * acc[mi][ni][q];
+}
+
 }  // namespace erebus
