@@ -99,29 +99,46 @@ __global__ void k_mf_pad(MfView V, int nfronts) {
 // ---------------------------------------------------------------------------
 
 // Tile (I, J) of front f += the children's Schur complement entries that
-// map onto it (child 0 first, then child 1).
-__device__ void mf_extend_add_tile(const MfView &V, const MfFront &f, int I, int J) {
-    double *T = ftile(V, f, I, J);
+// map onto it (child 0 first, then child 1).  The tile's row and column maps
+// are staged in shared memory; a child that maps onto no row or no column
+// of the tile is skipped, and so is the whole tile when neither child does.
+__device__ void mf_extend_add_tile(const MfView &V, const MfFront &f, int I, int J,
+                                   int (*emap)[64]) {
     const int *map = V.eamap + f.map_off;
-    MfFront C0, C1;
-    bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
-    if (h0) C0 = V.fr[f.c0];
-    if (h1) C1 = V.fr[f.c1];
-#pragma unroll 4
-    for (int q = 0; q < 16; q++) {
-        int e = threadIdx.x + 256 * q, r = e & 63, c = e >> 6;
-        int a = I * 64 + r, b = J * 64 + c;
-        double s = __ldcg(&T[c * 64 + r]);
-        if (h0) {
-            int ia = __ldg(&map[2 * a]), ib = __ldg(&map[2 * b]);
-            if (ia >= 0 && ib >= 0) s += __ldcg(V.F + felem(C0, C0.Kp + ia, C0.Kp + ib));
-        }
-        if (h1) {
-            int ia = __ldg(&map[2 * a + 1]), ib = __ldg(&map[2 * b + 1]);
-            if (ia >= 0 && ib >= 0) s += __ldcg(V.F + felem(C1, C1.Kp + ia, C1.Kp + ib));
-        }
-        T[c * 64 + r] = s;
+    const int tid = threadIdx.x;
+    if (tid < 128) {
+        int a = (tid < 64 ? I : J) * 64 + (tid & 63);
+        emap[tid < 64 ? 0 : 2][tid & 63] = __ldg(&map[2 * a]);
+        emap[tid < 64 ? 1 : 3][tid & 63] = __ldg(&map[2 * a + 1]);
     }
+    __syncthreads();
+    const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
+    const int lane64 = tid & 63, which = tid >> 6;   // 4 groups of 64 threads
+    int any = which < 4 && emap[which][lane64] >= 0;
+    int r0 = __syncthreads_or(which == 0 && any), c0 = __syncthreads_or(which == 2 && any);
+    int r1 = __syncthreads_or(which == 1 && any), c1 = __syncthreads_or(which == 3 && any);
+    const bool u0 = h0 && r0 && c0, u1 = h1 && r1 && c1;
+    if (u0 || u1) {
+        double *T = ftile(V, f, I, J);
+        MfFront C0, C1;
+        if (u0) C0 = V.fr[f.c0];
+        if (u1) C1 = V.fr[f.c1];
+#pragma unroll 4
+        for (int q = 0; q < 16; q++) {
+            int e = tid + 256 * q, r = e & 63, c = e >> 6;
+            double s = __ldcg(&T[c * 64 + r]);
+            if (u0) {
+                int ia = emap[0][r], ib = emap[2][c];
+                if (ia >= 0 && ib >= 0) s += __ldcg(V.F + felem(C0, C0.Kp + ia, C0.Kp + ib));
+            }
+            if (u1) {
+                int ia = emap[1][r], ib = emap[3][c];
+                if (ia >= 0 && ib >= 0) s += __ldcg(V.F + felem(C1, C1.Kp + ia, C1.Kp + ib));
+            }
+            T[c * 64 + r] = s;
+        }
+    }
+    __syncthreads();
 }
 
 // Inverts tile T in place (Gauss-Jordan in the FFMA register layout).
@@ -176,12 +193,22 @@ __device__ void mf_update_tile(const MfView &V, const MfFront &f, int I, int J, 
     __syncthreads();
 }
 
+// Fronts of a level whose tile counts a CTA keeps in shared memory; levels
+// with more fronts run one front per CTA.
+constexpr int MF_KM_MAX = 256;
+
+struct MfFactorSmem {
+    MmaSmem m;
+    int emap[4][64];
+    int2 km[MF_KM_MAX];   // (Kt, Mt) of the level's fronts
+};
+
 // Number of update tasks of step K: rows/cols K+1..Mt-1 except the block
 // of update rows and update columns (deferred to the Schur phase).
-__device__ __forceinline__ int mf_nupd(const MfFront &f, int K) {
-    if (K >= f.Kt) return 0;
-    int R = f.Mt - K - 1, e = f.Kt - K - 1;
-    return e * R + (f.Mt - f.Kt) * e;
+__device__ __forceinline__ int mf_nupd(int Kt, int Mt, int K) {
+    if (K >= Kt) return 0;
+    int R = Mt - K - 1, e = Kt - K - 1;
+    return e * R + (Mt - Kt) * e;
 }
 __device__ __forceinline__ void mf_upd_ij(const MfFront &f, int K, int u, int &I, int &J) {
     int R = f.Mt - K - 1, e = f.Kt - K - 1;
@@ -197,16 +224,19 @@ __device__ __forceinline__ void mf_upd_ij(const MfFront &f, int K, int u, int &I
 }
 
 // The whole partial LU of one front by one CTA.
-__device__ void mf_factor_local(const MfView &V, const MfFront &f, MmaSmem &S, int *err) {
+__device__ void mf_factor_local(const MfView &V, const MfFront &f, MfFactorSmem &FS,
+                                int *err) {
+    MmaSmem &S = FS.m;
     if (f.c0 >= 0 || f.c1 >= 0) {
-        for (int t = 0; t < f.Mt * f.Mt; t++) mf_extend_add_tile(V, f, t % f.Mt, t / f.Mt);
+        for (int t = 0; t < f.Mt * f.Mt; t++)
+            mf_extend_add_tile(V, f, t % f.Mt, t / f.Mt, FS.emap);
         __threadfence_block();
         __syncthreads();
     }
     for (int K = 0; K < f.Kt; K++) {
         if (K == 0) mf_invert_tile(ftile(V, f, 0, 0), S, err);
         for (int I = K + 1; I < f.Mt; I++) mf_l_tile(V, f, I, K, S);
-        int nu = mf_nupd(f, K);
+        int nu = mf_nupd(f.Kt, f.Mt, K);
         for (int u = 0; u < nu; u++) {
             int I, J;
             mf_upd_ij(f, K, u, I, J);
@@ -217,57 +247,71 @@ __device__ void mf_factor_local(const MfView &V, const MfFront &f, MmaSmem &S, i
         for (int I = f.Kt; I < f.Mt; I++) mf_update_tile(V, f, I, J, 0, f.Kt, S, err, false);
 }
 
-// Runs task(f, u) for the tasks u in [0, count(f)) of the fronts [fb, fe),
-// numbered consecutively across the fronts and dealt round-robin to CTAs.
+// Runs task(f, u) for the tasks u in [0, count(Kt, Mt)) of the fronts
+// [fb, fe), numbered consecutively across the fronts and dealt round-robin
+// to the CTAs.  km holds (Kt, Mt) of the fronts in shared memory; a front's
+// descriptor is read only when this CTA has one of its tasks.
 template <class Count, class Task>
-__device__ void mf_for_tasks(const MfView &V, int fb, int fe, Count count, Task task) {
+__device__ void mf_for_tasks(const MfView &V, int fb, int fe, const int2 *km, Count count,
+                             Task task) {
     const int G = gridDim.x, me = blockIdx.x;
     long long base = 0;
     for (int fi = fb; fi < fe; fi++) {
-        const MfFront f = V.fr[fi];
-        int cnt = count(f);
+        int2 q = km[fi - fb];
+        int cnt = count(q.x, q.y);
         if (cnt <= 0) continue;
         int first = (int)(((me - base) % G + G) % G);
-        for (int u = first; u < cnt; u += G) task(f, u);
+        if (first < cnt) {
+            const MfFront f = V.fr[fi];
+            for (int u = first; u < cnt; u += G) task(f, u);
+        }
         base += cnt;
     }
+}
+
+// (Kt, Mt) of the fronts [fb, fe) into shared memory.
+__device__ __forceinline__ void mf_load_km(const MfView &V, int fb, int fe, int2 *km) {
+    for (int i = threadIdx.x; i < fe - fb; i += blockDim.x) {
+        const MfFront &f = V.fr[fb + i];
+        km[i] = make_int2(f.Kt, f.Mt);
+    }
+    __syncthreads();
 }
 
 __global__ void __launch_bounds__(LU_THREADS, 2)
 k_mf_factor(MfView V, unsigned int *bar, int *err) {
     extern __shared__ __align__(16) double smem_raw[];
-    MmaSmem &S = *reinterpret_cast<MmaSmem *>(smem_raw);
+    MfFactorSmem &FS = *reinterpret_cast<MfFactorSmem *>(smem_raw);
+    MmaSmem &S = FS.m;
     const int G = gridDim.x;
     for (int p = 0; p < V.nlev; p++) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
-        if (fe - fb >= G / 2) {
+        if (fe - fb >= G / 2 || fe - fb > MF_KM_MAX) {
             for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
                 const MfFront f = V.fr[fi];
-                mf_factor_local(V, f, S, err);
+                mf_factor_local(V, f, FS, err);
             }
             grid_barrier(bar, err);
             continue;
         }
+        mf_load_km(V, fb, fe, FS.km);
         // extend-add; the task of tile (0,0) also inverts it
         mf_for_tasks(
-            V, fb, fe, [](const MfFront &f) { return f.Mt * f.Mt; },
+            V, fb, fe, FS.km, [](int, int Mt) { return Mt * Mt; },
             [&](const MfFront &f, int u) {
                 int I = u % f.Mt, J = u / f.Mt;
-                if (f.c0 >= 0 || f.c1 >= 0) {
-                    mf_extend_add_tile(V, f, I, J);
-                    __syncthreads();
-                }
+                if (f.c0 >= 0 || f.c1 >= 0) mf_extend_add_tile(V, f, I, J, FS.emap);
                 if (u == 0 && f.Kt > 0) mf_invert_tile(ftile(V, f, 0, 0), S, err);
             });
         grid_barrier(bar, err);
         const int ktmax = V.lvl_kt[p];
         for (int K = 0; K < ktmax; K++) {
             mf_for_tasks(
-                V, fb, fe, [K](const MfFront &f) { return K < f.Kt ? f.Mt - K - 1 : 0; },
+                V, fb, fe, FS.km, [K](int Kt, int Mt) { return K < Kt ? Mt - K - 1 : 0; },
                 [&](const MfFront &f, int u) { mf_l_tile(V, f, K + 1 + u, K, S); });
             grid_barrier(bar, err);
             mf_for_tasks(
-                V, fb, fe, [K](const MfFront &f) { return mf_nupd(f, K); },
+                V, fb, fe, FS.km, [K](int Kt, int Mt) { return mf_nupd(Kt, Mt, K); },
                 [&](const MfFront &f, int u) {
                     int I, J;
                     mf_upd_ij(f, K, u, I, J);
@@ -276,7 +320,7 @@ k_mf_factor(MfView V, unsigned int *bar, int *err) {
             grid_barrier(bar, err);
         }
         mf_for_tasks(
-            V, fb, fe, [](const MfFront &f) { return (f.Mt - f.Kt) * (f.Mt - f.Kt); },
+            V, fb, fe, FS.km, [](int Kt, int Mt) { return (Mt - Kt) * (Mt - Kt); },
             [&](const MfFront &f, int u) {
                 int ru = f.Mt - f.Kt;
                 mf_update_tile(V, f, f.Kt + u % ru, f.Kt + u / ru, 0, f.Kt, S, err, false);
@@ -292,6 +336,7 @@ struct MfSolveSmem {
     double x[8][64];       // per-warp vector pieces
     double part[8][64];    // per-warp partial sums
     double y[64];
+    int2 km[MF_KM_MAX];    // (Kt, Mt) of the level's fronts
 };
 
 // lane's rows r0 = lane, r1 = lane + 32 of T x (T a 64 x 64 column-major
@@ -425,7 +470,8 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
     // forward: leaves to root
     for (int p = 0; p < V.nlev; p++) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
-        const bool local = fe - fb >= G / 2;
+        const bool local = fe - fb >= G / 2 || fe - fb > MF_KM_MAX;
+        if (!local) mf_load_km(V, fb, fe, S.km);
         for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
             const MfFront f = V.fr[fi];
             double *v = V.vec + f.vec_off;
@@ -437,7 +483,7 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
             grid_barrier(bar, err);
             // update rows: v_I -= sum_{K < Kt} L_IK y_K
             mf_for_tasks(
-                V, fb, fe, [](const MfFront &f) { return f.Mt - f.Kt; },
+                V, fb, fe, S.km, [](int Kt, int Mt) { return Mt - Kt; },
                 [&](const MfFront &f, int u) {
                     double *v = V.vec + f.vec_off;
                     mf_row_gemv(V, f, v, f.Kt + u, 0, f.Kt,
@@ -449,7 +495,8 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
     // backward: root to leaves
     for (int p = V.nlev - 1; p >= 0; p--) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
-        const bool local = fe - fb >= G / 2;
+        const bool local = fe - fb >= G / 2 || fe - fb > MF_KM_MAX;
+        if (!local) mf_load_km(V, fb, fe, S.km);
         auto ring_x = [&](const MfFront &f) {
             const int *var = V.vars + f.var_off;
             return [=](int J, int c) {
@@ -460,7 +507,7 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
         if (!local) {
             // eliminated rows: v_K -= sum_{J >= Kt} U_KJ x_J
             mf_for_tasks(
-                V, fb, fe, [](const MfFront &f) { return f.Mt > f.Kt ? f.Kt : 0; },
+                V, fb, fe, S.km, [](int Kt, int Mt) { return Mt > Kt ? Kt : 0; },
                 [&](const MfFront &f, int u) {
                     mf_row_gemv(V, f, V.vec + f.vec_off, u, f.Kt, f.Mt, ring_x(f), S);
                 });
@@ -590,7 +637,7 @@ int mf_factor(erebus_state *s, BandSystem &sys) {
                   sys.err);
     int nf = (int)D.plan.fronts.size();
     EREBUS_LAUNCH(s, k_mf_pad, nf, 64, 0, V, nf);
-    size_t smem = sizeof(MmaSmem);
+    size_t smem = sizeof(MfFactorSmem);
     cudaFuncSetAttribute(k_mf_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int blocks = mf_blocks(s, (const void *)k_mf_factor, smem);
     if (blocks < 1) {
