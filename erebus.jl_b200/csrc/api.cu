@@ -287,6 +287,7 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
     s->r_dH = (double *)alloc(cap * 8);
     s->r_flag = (int8_t *)alloc(cap);
     s->tmp_node = (double *)alloc(2 * np * 8);
+    s->norm_part = (double *)alloc(2 * 1024 * 8);
     size_t na = (size_t)g.Nxm * g.Nym;
     s->a_mdis = (unsigned long long *)alloc(na * 8);
     s->a_mnum = (int *)alloc(na * 4);
@@ -294,7 +295,7 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
     s->a_rank = (int *)alloc(na * 4);
     s->a_flag = (int *)alloc(na * 4);
     s->dsc = (DevScalars *)alloc(sizeof(DevScalars));
-    if (!s->r_dM || !s->r_dH || !s->r_flag || !s->tmp_node || !s->a_mdis || !s->a_mnum ||
+    if (!s->r_dM || !s->r_dH || !s->r_flag || !s->tmp_node || !s->norm_part || !s->a_mdis || !s->a_mnum ||
         !s->a_src || !s->a_rank || !s->a_flag || !s->dsc)
         return fail(EREBUS_ENOMEM, "scratch");
     if (cudaMallocHost(&s->hsc, sizeof(DevScalars)) != cudaSuccess)

@@ -117,6 +117,7 @@ struct erebus_state {
     double *r_dM = nullptr, *r_dH = nullptr;   // per-marker reaction outputs
     int8_t *r_flag = nullptr;
     double *tmp_node = nullptr;                // node-sized scratch
+    double *norm_part = nullptr;               // partial sums of the residual norms
     double *partials = nullptr;                // reduction partials
     // replenishment scratch (per marker-grid anchor)
     unsigned long long *a_mdis = nullptr;

@@ -174,6 +174,71 @@ static __device__ void tile_inverse(double a[4][4], double *vec, int *err) {
     __syncthreads();
 }
 
+// In-place Gauss-Jordan inverse (no pivoting) of the tile held in registers
+// `a` (FFMA layout), eliminating two unknowns per step with the inverse of
+// their 2 x 2 pivot block: for pivot rows/columns K = {k, k+1},
+//   A_ij -= A_iK P^{-1} A_Kj,  A_iK <- -A_iK P^{-1},  A_Kj <- P^{-1} A_Kj,
+//   A_KK <- P^{-1}.
+// One barrier per step (32 steps); `vec` holds 2 x 4 x 64 doubles.  A zero
+// or non-finite pivot determinant raises *err = 2.
+static __device__ void tile_inverse2(double a[4][4], double *vec, int *err) {
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+#pragma unroll
+    for (int kq = 0; kq < 4; kq++)
+        for (int kk = 0; kk < 16; kk += 2) {
+            const int k = kq * 16 + kk;
+            double *buf = vec + ((k >> 1) & 1) * 4 * NB_TILE;
+            double *col0 = buf, *col1 = buf + NB_TILE, *row0 = buf + 2 * NB_TILE,
+                   *row1 = buf + 3 * NB_TILE;
+            if (tx == kk || tx == kk + 1) {
+                double *cd = tx == kk ? col0 : col1;
+#pragma unroll
+                for (int i = 0; i < 4; i++) cd[ty + 16 * i] = a[i][kq];
+            }
+            if (ty == kk || ty == kk + 1) {
+                double *rd = ty == kk ? row0 : row1;
+#pragma unroll
+                for (int j = 0; j < 4; j++) rd[tx + 16 * j] = a[kq][j];
+            }
+            __syncthreads();
+            const double p00 = row0[k], p01 = row0[k + 1], p10 = row1[k], p11 = row1[k + 1];
+            const double det = p00 * p11 - p01 * p10;
+            if (threadIdx.x == 0 && !(fabs(det) > 0.0 && fabs(det) < INFINITY)) atomicExch(err, 2);
+            const double id = 1.0 / det;
+            const double q00 = p11 * id, q01 = -p01 * id, q10 = -p10 * id, q11 = p00 * id;
+            double u0[4], u1[4], r0[4], r1[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                double c0 = col0[ty + 16 * i], c1 = col1[ty + 16 * i];
+                u0[i] = c0 * q00 + c1 * q10;
+                u1[i] = c0 * q01 + c1 * q11;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                r0[j] = row0[tx + 16 * j];
+                r1[j] = row1[tx + 16 * j];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    a[i][j] = fma(-u0[i], r0[j], fma(-u1[i], r1[j], a[i][j]));
+            // pivot columns, then pivot rows, then the pivot block
+            if (tx == kk || tx == kk + 1) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) a[i][kq] = tx == kk ? -u0[i] : -u1[i];
+            }
+            if (ty == kk || ty == kk + 1) {
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    a[kq][j] = ty == kk ? q00 * r0[j] + q01 * r1[j] : q10 * r0[j] + q11 * r1[j];
+                if (tx == kk || tx == kk + 1)
+                    a[kq][kq] = ty == kk ? (tx == kk ? q00 : q01) : (tx == kk ? q10 : q11);
+            }
+        }
+    __syncthreads();
+}
+
 struct FactorSmem {
     double As[STILE], Bt[STILE], Cs[STILE];
     double vec[2 * 2 * NB_TILE];
@@ -197,7 +262,7 @@ constexpr int MMA_STAGE = MMA_KC * MMA_LA + NB_TILE * MMA_LB;   // doubles per s
 
 struct MmaSmem {
     double stage[MMA_NSTAGE][MMA_STAGE];
-    double vec[2 * 2 * NB_TILE];
+    double vec[2 * 4 * NB_TILE];   // pivot rows/columns of tile_inverse2, double-buffered
 };
 static_assert(MMA_STAGE >= STILE, "a stage holds a padded tile");
 
