@@ -294,9 +294,10 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
     s->a_src = (int *)alloc(na * 4);
     s->a_rank = (int *)alloc(na * 4);
     s->a_flag = (int *)alloc(na * 4);
+    s->a_part = (int *)alloc((na / 1024 + 2) * 4);
     s->dsc = (DevScalars *)alloc(sizeof(DevScalars));
     if (!s->r_dM || !s->r_dH || !s->r_flag || !s->tmp_node || !s->norm_part || !s->a_mdis || !s->a_mnum ||
-        !s->a_src || !s->a_rank || !s->a_flag || !s->dsc)
+        !s->a_src || !s->a_rank || !s->a_flag || !s->a_part || !s->dsc)
         return fail(EREBUS_ENOMEM, "scratch");
     if (cudaMallocHost(&s->hsc, sizeof(DevScalars)) != cudaSuccess)
         return fail(EREBUS_ENOMEM, "pinned scalars");

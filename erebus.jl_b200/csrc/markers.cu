@@ -906,28 +906,63 @@ __global__ void k_repl_search(Geo g, int dii, int djj, const double *xm, const d
     flag[a] = bm >= 0;
 }
 
-// Exclusive scan of the anchor flags in anchor order (single block).
-__global__ void k_repl_scan(const int *flag, int *rank, int na, DevScalars *sc) {
-    __shared__ int part[1024];
-    int T = blockDim.x, t = threadIdx.x;
-    int chunk = (na + T - 1) / T;
-    int lo = t * chunk, hi = min(na, lo + chunk);
-    int sum = 0;
-    for (int k = lo; k < hi; k++) sum += flag[k];
-    part[t] = sum;
+// Exclusive scan of the anchor flags in anchor order, in three passes over
+// tiles of SCAN_B anchors: tile sums, a scan of the tile sums (one block;
+// also the number of new markers), and the scan inside each tile.
+constexpr int SCAN_B = 1024;
+
+// exclusive prefix of v over the SCAN_B threads of the block; *total = sum
+__device__ int block_exclusive_scan(int v, int *wsum, int *total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
     __syncthreads();
-    for (int off = 1; off < T; off <<= 1) {
-        int v = t >= off ? part[t - off] : 0;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
+    if (w == 0) {
+        int s = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        wsum[lane] = s;   // inclusive warp-total prefix
     }
-    int run = part[t] - sum;
-    for (int k = lo; k < hi; k++) {
-        rank[k] = run;
-        run += flag[k];
+    __syncthreads();
+    int excl = x - v + (w > 0 ? wsum[w - 1] : 0);
+    *total = wsum[31];
+    __syncthreads();
+    return excl;
+}
+
+__global__ void k_repl_tile_sums(const int *flag, int na, int *part) {
+    __shared__ int wsum[32];
+    int k = blockIdx.x * SCAN_B + threadIdx.x, tot;
+    block_exclusive_scan(k < na ? flag[k] : 0, wsum, &tot);
+    if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+__global__ void k_repl_scan_tiles(int *part, int ntiles, DevScalars *sc) {
+    __shared__ int wsum[32];
+    int carry = 0;
+    for (int b = 0; b < ntiles; b += SCAN_B) {
+        int k = b + threadIdx.x, tot;
+        int v = k < ntiles ? part[k] : 0;
+        int e = block_exclusive_scan(v, wsum, &tot);
+        if (k < ntiles) part[k] = carry + e;
+        carry += tot;
     }
-    if (t == T - 1) sc->repl_count = part[T - 1];
+    if (threadIdx.x == 0) sc->repl_count = carry;
+}
+
+__global__ void k_repl_scan(const int *flag, int na, const int *part, int *rank) {
+    __shared__ int wsum[32];
+    int k = blockIdx.x * SCAN_B + threadIdx.x, tot;
+    int e = block_exclusive_scan(k < na ? flag[k] : 0, wsum, &tot);
+    if (k < na) rank[k] = part[blockIdx.x] + e;
 }
 
 __global__ void k_repl_append(ErebusParams p, Geo g, MP M, const int *src, const int *flag,
@@ -965,7 +1000,10 @@ int replenish(erebus_state *s, int timestep, int64_t *marknum) {
     }
     EREBUS_LAUNCH(s, k_repl_search, nblocks(na), kThreads, 0, g, 5 * s->p.Nymc,
                   5 * s->p.Nxmc, s->m[M_xm], s->m[M_ym], s->a_mnum, s->a_src, flag);
-    EREBUS_LAUNCH(s, k_repl_scan, 1, 1024, 0, flag, s->a_rank, na, s->dsc);
+    int ntiles = (int)((na + SCAN_B - 1) / SCAN_B);
+    EREBUS_LAUNCH(s, k_repl_tile_sums, ntiles, SCAN_B, 0, flag, (int)na, s->a_part);
+    EREBUS_LAUNCH(s, k_repl_scan_tiles, 1, SCAN_B, 0, s->a_part, ntiles, s->dsc);
+    EREBUS_LAUNCH(s, k_repl_scan, ntiles, SCAN_B, 0, flag, (int)na, s->a_part, s->a_rank);
     EREBUS_LAUNCH(s, k_repl_append, nblocks(na), kThreads, 0, s->p, g, mptr(s), s->a_src,
                   flag, s->a_rank, n, s->capacity, s->dsc, timestep);
     int rc = check_cuda(s, cudaMemcpyAsync(&s->hsc->repl_count, &s->dsc->repl_count,

@@ -123,19 +123,31 @@ __device__ void mf_extend_add_tile(const MfView &V, const MfFront &f, int I, int
         MfFront C0, C1;
         if (u0) C0 = V.fr[f.c0];
         if (u1) C1 = V.fr[f.c1];
-#pragma unroll 4
-        for (int q = 0; q < 16; q++) {
-            int e = tid + 256 * q, r = e & 63, c = e >> 6;
-            double s = __ldcg(&T[c * 64 + r]);
-            if (u0) {
-                int ia = emap[0][r], ib = emap[2][c];
-                if (ia >= 0 && ib >= 0) s += __ldcg(V.F + felem(C0, C0.Kp + ia, C0.Kp + ib));
+        // all loads of a batch are issued before any store (the stores could
+        // alias the children's storage as far as the compiler knows)
+#pragma unroll 1
+        for (int q0 = 0; q0 < 16; q0 += 8) {
+            double t[8], x0[8], x1[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                int e = tid + 256 * (q0 + q), r = e & 63, c = e >> 6;
+                t[q] = __ldcg(&T[c * 64 + r]);
+                x0[q] = 0.0;
+                x1[q] = 0.0;
+                if (u0) {
+                    int ia = emap[0][r], ib = emap[2][c];
+                    if (ia >= 0 && ib >= 0) x0[q] = __ldcg(V.F + felem(C0, C0.Kp + ia, C0.Kp + ib));
+                }
+                if (u1) {
+                    int ia = emap[1][r], ib = emap[3][c];
+                    if (ia >= 0 && ib >= 0) x1[q] = __ldcg(V.F + felem(C1, C1.Kp + ia, C1.Kp + ib));
+                }
             }
-            if (u1) {
-                int ia = emap[1][r], ib = emap[3][c];
-                if (ia >= 0 && ib >= 0) s += __ldcg(V.F + felem(C1, C1.Kp + ia, C1.Kp + ib));
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                int e = tid + 256 * (q0 + q), r = e & 63, c = e >> 6;
+                T[c * 64 + r] = (t[q] + x0[q]) + x1[q];
             }
-            T[c * 64 + r] = s;
         }
     }
     __syncthreads();
@@ -159,10 +171,9 @@ __device__ void mf_invert_tile(double *T, MmaSmem &S, int *err) {
 // L_IK = A_IK D_K^{-1} (tile (K,K) holds D_K^{-1})
 __device__ void mf_l_tile(const MfView &V, const MfFront &f, int I, int K, MmaSmem &S) {
     MmaAcc acc;
-    frag_zero(acc);
     const double *A = ftile(V, f, I, K), *B = ftile(V, f, K, K);
     mma_tiles(
-        S, 1, [&](int) { return A; }, [&](int) { return B; }, acc);
+        S, 1, [&](int) { return A; }, [&](int) { return B; }, acc, [&] { frag_zero(acc); });
     frag_store(ftile(V, f, I, K), acc, 1.0);
     __syncthreads();
 }
@@ -172,10 +183,10 @@ __device__ void mf_update_tile(const MfView &V, const MfFront &f, int I, int J, 
                                int k1, MmaSmem &S, int *err, bool invert) {
     MmaAcc acc;
     double *C = ftile(V, f, I, J);
-    frag_load(C, acc, -1.0);
     mma_tiles(
         S, k1 - k0, [&](int p) { return (const double *)ftile(V, f, I, k0 + p); },
-        [&](int p) { return (const double *)ftile(V, f, k0 + p, J); }, acc);
+        [&](int p) { return (const double *)ftile(V, f, k0 + p, J); }, acc,
+        [&] { frag_load(C, acc, -1.0); });
     if (invert) {
         double a[4][4];
         double *P = S.stage[0];

@@ -122,6 +122,7 @@ struct erebus_state {
     // replenishment scratch (per marker-grid anchor)
     unsigned long long *a_mdis = nullptr;
     int *a_mnum = nullptr, *a_src = nullptr, *a_rank = nullptr, *a_flag = nullptr;
+    int *a_part = nullptr;   // per-tile sums of the anchor-flag scan
 
     erebus::DevScalars *dsc = nullptr;    // device scalars
     erebus::DevScalars *hsc = nullptr;    // pinned host mirror

@@ -339,14 +339,17 @@ static __device__ __forceinline__ void mma_chunk(const double *st, MmaAcc acc) {
 
 // acc += sum_{p < np} tileA(p) * tileB(p) (global column-major tiles),
 // three-stage cp.async pipeline.  Ends with the stages free.
-template <class TA, class TB>
-static __device__ void mma_tiles(MmaSmem &S, int np, TA tileA, TB tileB, MmaAcc acc) {
+// `pre()` runs once the first copies are in flight (e.g. loading the
+// accumulator), so its latency overlaps theirs.
+template <class TA, class TB, class Pre>
+static __device__ void mma_tiles(MmaSmem &S, int np, TA tileA, TB tileB, MmaAcc acc, Pre pre) {
     const int nq = 2 * np;
 #pragma unroll 1
     for (int q = 0; q < 2; q++) {
         if (q < nq) mma_load_chunk(S.stage[q], tileA(q >> 1), tileB(q >> 1), q & 1);
         cp_async_commit();
     }
+    pre();
 #pragma unroll 1
     for (int q = 0; q < nq; q++) {
         cp_async_wait1();
