@@ -343,52 +343,103 @@ k_mf_factor(MfView V, unsigned int *bar, int *err) {
 // ---------------------------------------------------------------------------
 // solve
 // ---------------------------------------------------------------------------
+// The solve streams factor tiles into shared memory with bulk async copies
+// (one 32 KB copy per tile, MF_SLOTS tiles in flight per CTA) and computes
+// from there: the sweeps read every tile once, so their speed is the rate at
+// which a CTA keeps HBM reads in flight.
+constexpr int MF_SLOTS = 3;
+
 struct MfSolveSmem {
-    double x[8][64];       // per-warp vector pieces
-    double part[8][64];    // per-warp partial sums
+    double tile[MF_SLOTS][T2];
+    unsigned long long bar[MF_SLOTS];
+    double part[4][64];    // quarter partial sums
+    double x[64];          // vector piece the current tile multiplies
     double y[64];
     int2 km[MF_KM_MAX];    // (Kt, Mt) of the level's fronts
 };
 
-// lane's rows r0 = lane, r1 = lane + 32 of T x (T a 64 x 64 column-major
-// tile in global memory, x in shared memory)
-__device__ __forceinline__ void warp_tile_gemv(const double *T, const double *x, double &s0,
-                                               double &s1) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll 8
-    for (int c = 0; c < 64; c++) {
-        double xc = x[c];
-        s0 = fma(__ldcg(&T[c * 64 + lane]), xc, s0);
-        s1 = fma(__ldcg(&T[c * 64 + lane + 32]), xc, s1);
+__device__ __forceinline__ uint32_t mf_smem(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Issues the copy of one 64 x 64 tile into slot `sl` (thread 0).
+__device__ __forceinline__ void mf_fetch(MfSolveSmem &S, int sl, const double *src) {
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                         mf_smem(&S.bar[sl])),
+                     "r"((uint32_t)(T2 * sizeof(double)))
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(mf_smem(S.tile[sl])),
+            "l"(src), "r"((uint32_t)(T2 * sizeof(double))), "r"(mf_smem(&S.bar[sl]))
+            : "memory");
     }
 }
 
-// v[I] -= sum_{K in ks} T(I, K) v[K] for one target tile row I, the K range
-// split over the 8 warps, partial sums reduced through shared memory.
-// `xsrc(K, c)` gives element c of the vector piece K.
-template <class Xsrc>
-__device__ void mf_row_gemv(const MfView &V, const MfFront &f, double *v, int I, int k0, int k1,
-                            Xsrc xsrc, MfSolveSmem &S) {
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// Waits (bounded, 2 s) for phase `parity` of slot `sl`; on timeout *err = 3.
+__device__ __forceinline__ void mf_slot_wait(MfSolveSmem &S, int sl, uint32_t parity, int *err) {
+    uint32_t ok;
+    unsigned long long t0 = 0;
+    for (int spin = 0;; spin++) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(mf_smem(&S.bar[sl])), "r"(parity)
+            : "memory");
+        if (ok) return;
+        if (spin == 0) t0 = globaltimer();
+        else if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
+            atomicExch(err, 3);
+            return;
+        }
+    }
+}
+
+// Streams the n tiles src(0..n-1) through the slots and calls use(i, tile)
+// with all threads once tile i is in shared memory.  uses[] counts the
+// phases of each slot's barrier (identical in every thread).
+template <class Src, class Use>
+__device__ void mf_stream(MfSolveSmem &S, uint32_t *uses, int n, Src src, Use use, int *err) {
+    for (int i = 0; i < n && i < MF_SLOTS; i++) mf_fetch(S, i, src(i));
+    for (int i = 0; i < n; i++) {
+        const int sl = i % MF_SLOTS;
+        mf_slot_wait(S, sl, uses[sl] & 1u, err);
+        uses[sl]++;
+        use(i, S.tile[sl]);
+        __syncthreads();
+        if (i + MF_SLOTS < n) mf_fetch(S, sl, src(i + MF_SLOTS));
+    }
+}
+
+// Thread (r, q) = (tid % 64, tid / 64): its share of row r of T x, columns
+// 16 q .. 16 q + 15 (T in shared memory, column-major; x in shared memory).
+__device__ __forceinline__ double mf_quarter(const double *T, const double *x) {
+    const int r = threadIdx.x & 63, q = threadIdx.x >> 6;
+    const double *t = T + q * 16 * 64 + r;
+    const double *xx = x + q * 16;
     double s0 = 0.0, s1 = 0.0;
-    for (int K = k0 + w; K < k1; K += 8) {
-        S.x[w][lane] = xsrc(K, lane);
-        S.x[w][lane + 32] = xsrc(K, lane + 32);
-        __syncwarp();
-        warp_tile_gemv(ftile(V, f, I, K), S.x[w], s0, s1);
-        __syncwarp();
-    }
-    S.part[w][lane] = s0;
-    S.part[w][lane + 32] = s1;
-    __syncthreads();
-    if (threadIdx.x < 64) {
-        double s = 0.0;
 #pragma unroll
-        for (int q = 0; q < 8; q++) s += S.part[q][threadIdx.x];
-        double *d = &v[I * 64 + threadIdx.x];
-        __stcg(d, __ldcg(d) - s);
+    for (int c = 0; c < 16; c += 2) {
+        s0 = fma(t[c * 64], xx[c], s0);
+        s1 = fma(t[(c + 1) * 64], xx[c + 1], s1);
+    }
+    return s0 + s1;
+}
+
+// Reduces the quarter sums s of all threads: returns the row total in
+// threads 0..63 (row = tid).  Ends with a barrier.
+__device__ __forceinline__ double mf_reduce_rows(MfSolveSmem &S, double s) {
+    S.part[threadIdx.x >> 6][threadIdx.x & 63] = s;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x < 64) {
+        const int r = threadIdx.x;
+        t = (S.part[0][r] + S.part[1][r]) + (S.part[2][r] + S.part[3][r]);
     }
     __syncthreads();
+    return t;
 }
 
 // Gathers the front vector: the right-hand side of the eliminated unknowns
@@ -412,72 +463,136 @@ __device__ void mf_gather_fwd(const MfView &V, const MfFront &f, const double *w
         }
         __stcg(&v[a], s);
     }
+    __syncthreads();
 }
 
-// Forward elimination inside the front: for K < Kt, rows I in (K, iend)
-// get v_I -= L_IK v_K; the warps take different rows.
+// Forward elimination inside a front: for each block column K < Kt, rows
+// I in (K, iend) get v_I -= L_IK y_K, with y_K = v_K final once column K
+// starts.  The tiles stream in column order.
 __device__ void mf_fwd_front(const MfView &V, const MfFront &f, double *v, int iend,
-                             MfSolveSmem &S) {
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int K = 0; K < f.Kt; K++) {
-        if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
-        __syncthreads();
-        for (int I = K + 1 + w; I < iend; I += 8) {
-            double s0 = 0.0, s1 = 0.0;
-            warp_tile_gemv(ftile(V, f, I, K), S.y, s0, s1);
-            double *d = &v[I * 64];
-            __stcg(&d[lane], __ldcg(&d[lane]) - s0);
-            __stcg(&d[lane + 32], __ldcg(&d[lane + 32]) - s1);
+                             MfSolveSmem &S, uint32_t *uses, int *err) {
+    // tile i -> (K, I): columns K = 0.. with iend - K - 1 tiles each
+    int n = 0;
+    for (int K = 0; K < f.Kt; K++) n += max(0, iend - K - 1);
+    int K = 0, I = 1;     // position of the next tile handed to use()
+    int fk = 0, fi = 1;   // position of the next tile fetched by src()
+    auto src = [&](int) {
+        while (fi >= iend) {
+            fk++;
+            fi = fk + 1;
         }
-        __syncthreads();
-    }
+        const double *t = ftile(V, f, fi, fk);
+        fi++;
+        return t;
+    };
+    mf_stream(
+        S, uses, n, src,
+        [&](int, const double *T) {
+            while (I >= iend) {
+                K++;
+                I = K + 1;
+            }
+            if (I == K + 1) {   // first tile of column K: y_K
+                if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
+                __syncthreads();
+            }
+            double t = mf_reduce_rows(S, mf_quarter(T, S.y));
+            if (threadIdx.x < 64) {
+                double *d = &v[I * 64 + threadIdx.x];
+                __stcg(d, __ldcg(d) - t);
+            }
+            I++;
+        },
+        err);
 }
 
-// Backward substitution inside the front (the update part already
-// subtracted): x_K = D_K^{-1} v_K, then v_I -= U_IK x_K for I < K; the
-// solution goes to v and to w.
-__device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, double *wout,
-                             MfSolveSmem &S) {
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int *var = V.vars + f.var_off;
-    for (int K = f.Kt - 1; K >= 0; K--) {
-        if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
-        __syncthreads();
-        // x_K = D^{-1} y: four column quarters per row, reduced in part
-        {
-            const double *Di = ftile(V, f, K, K);
-            int r = threadIdx.x & 63, q = threadIdx.x >> 6;
-            double s = 0.0;
-#pragma unroll 4
-            for (int c = q * 16; c < q * 16 + 16; c++) s = fma(__ldcg(&Di[c * 64 + r]), S.y[c], s);
-            S.part[q][r] = s;
-        }
-        __syncthreads();
-        if (threadIdx.x < 64) {
-            int r = threadIdx.x;
-            double x = (S.part[0][r] + S.part[1][r]) + (S.part[2][r] + S.part[3][r]);
-            S.x[0][r] = x;
-            __stcg(&v[K * 64 + r], x);
-            int a = K * 64 + r;
-            if (a < f.k) __stcg(&wout[var[a]], x);
-        }
-        __syncthreads();
-        for (int I = w; I < K; I += 8) {
-            double s0 = 0.0, s1 = 0.0;
-            warp_tile_gemv(ftile(V, f, I, K), S.x[0], s0, s1);
-            double *d = &v[I * 64];
-            __stcg(&d[lane], __ldcg(&d[lane]) - s0);
-            __stcg(&d[lane + 32], __ldcg(&d[lane + 32]) - s1);
-        }
-        __syncthreads();
+// v_I -= sum_{K in [k0, k1)} T(I, K) x_K for one tile row I; xsrc(K, c)
+// gives element c of the vector piece K.
+template <class Xsrc>
+__device__ void mf_row_gemv(const MfView &V, const MfFront &f, double *v, int I, int k0, int k1,
+                            Xsrc xsrc, MfSolveSmem &S, uint32_t *uses, int *err) {
+    double acc = 0.0;
+    mf_stream(
+        S, uses, k1 - k0, [&](int i) { return (const double *)ftile(V, f, I, k0 + i); },
+        [&](int i, const double *T) {
+            if (threadIdx.x < 64) S.x[threadIdx.x] = xsrc(k0 + i, threadIdx.x);
+            __syncthreads();
+            acc += mf_quarter(T, S.x);
+        },
+        err);
+    double t = mf_reduce_rows(S, acc);
+    if (threadIdx.x < 64) {
+        double *d = &v[I * 64 + threadIdx.x];
+        __stcg(d, __ldcg(d) - t);
     }
+    __syncthreads();
+}
+
+// Backward substitution inside a front (the update part already
+// subtracted): for K = Kt-1 .. 0, x_K = D_K^{-1} v_K, then v_I -= U_IK x_K
+// for I < K.  The solution goes to v and to w.  Tiles stream as (K,K),
+// (0,K), (1,K), ..., (K-1,K) for K descending.
+__device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, double *wout,
+                             MfSolveSmem &S, uint32_t *uses, int *err) {
+    const int *var = V.vars + f.var_off;
+    const int n = f.Kt * (f.Kt + 1) / 2;
+    int K = f.Kt - 1, j = 0;     // use position: j == 0 -> (K,K), else row j-1
+    int fk = f.Kt - 1, fj = 0;   // fetch position
+    auto src = [&](int) {
+        if (fj > fk) {
+            fk--;
+            fj = 0;
+        }
+        const double *t = fj == 0 ? ftile(V, f, fk, fk) : ftile(V, f, fj - 1, fk);
+        fj++;
+        return t;
+    };
+    mf_stream(
+        S, uses, n, src,
+        [&](int, const double *T) {
+            if (j > K) {
+                K--;
+                j = 0;
+            }
+            if (j == 0) {   // x_K = D_K^{-1} v_K
+                if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
+                __syncthreads();
+                double x = mf_reduce_rows(S, mf_quarter(T, S.y));
+                if (threadIdx.x < 64) {
+                    const int r = threadIdx.x, a = K * 64 + r;
+                    S.x[r] = x;
+                    __stcg(&v[a], x);
+                    if (a < f.k) __stcg(&wout[var[a]], x);
+                }
+                __syncthreads();
+            } else {        // v_I -= U_IK x_K, I = j - 1
+                double t = mf_reduce_rows(S, mf_quarter(T, S.x));
+                if (threadIdx.x < 64) {
+                    double *d = &v[(j - 1) * 64 + threadIdx.x];
+                    __stcg(d, __ldcg(d) - t);
+                }
+            }
+            j++;
+        },
+        err);
 }
 
 // Solves L U x = w in place (w: n values; rows >= n untouched).
 __global__ void __launch_bounds__(LU_THREADS, 2)
 k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
-    __shared__ MfSolveSmem S;
+    extern __shared__ __align__(128) double smem_raw[];
+    MfSolveSmem &S = *reinterpret_cast<MfSolveSmem *>(smem_raw);
     const int G = gridDim.x;
+    uint32_t uses[MF_SLOTS];
+    for (int i = 0; i < MF_SLOTS; i++) uses[i] = 0;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < MF_SLOTS; i++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mf_smem(&S.bar[i]))
+                         : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
     // forward: leaves to root
     for (int p = 0; p < V.nlev; p++) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
@@ -487,8 +602,7 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
             const MfFront f = V.fr[fi];
             double *v = V.vec + f.vec_off;
             mf_gather_fwd(V, f, w, v);
-            __syncthreads();
-            mf_fwd_front(V, f, v, local ? f.Mt : f.Kt, S);
+            mf_fwd_front(V, f, v, local ? f.Mt : f.Kt, S, uses, err);
         }
         if (!local) {
             grid_barrier(bar, err);
@@ -497,8 +611,9 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
                 V, fb, fe, S.km, [](int Kt, int Mt) { return Mt - Kt; },
                 [&](const MfFront &f, int u) {
                     double *v = V.vec + f.vec_off;
-                    mf_row_gemv(V, f, v, f.Kt + u, 0, f.Kt,
-                                [&](int K, int c) { return __ldcg(&v[K * 64 + c]); }, S);
+                    mf_row_gemv(
+                        V, f, v, f.Kt + u, 0, f.Kt,
+                        [&](int K, int c) { return __ldcg(&v[K * 64 + c]); }, S, uses, err);
                 });
         }
         grid_barrier(bar, err);
@@ -520,7 +635,8 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
             mf_for_tasks(
                 V, fb, fe, S.km, [](int Kt, int Mt) { return Mt > Kt ? Kt : 0; },
                 [&](const MfFront &f, int u) {
-                    mf_row_gemv(V, f, V.vec + f.vec_off, u, f.Kt, f.Mt, ring_x(f), S);
+                    mf_row_gemv(V, f, V.vec + f.vec_off, u, f.Kt, f.Mt, ring_x(f), S, uses,
+                                err);
                 });
             grid_barrier(bar, err);
         }
@@ -529,8 +645,8 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
             double *v = V.vec + f.vec_off;
             if (local)
                 for (int K = 0; K < f.Kt && f.Mt > f.Kt; K++)
-                    mf_row_gemv(V, f, v, K, f.Kt, f.Mt, ring_x(f), S);
-            mf_bwd_front(V, f, v, w, S);
+                    mf_row_gemv(V, f, v, K, f.Kt, f.Mt, ring_x(f), S, uses, err);
+            mf_bwd_front(V, f, v, w, S, uses, err);
         }
         grid_barrier(bar, err);
     }
@@ -696,7 +812,9 @@ int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
     }
     MfDevice &D = *sys.mf;
     MfView V = mf_view(D, sys);
-    int blocks = mf_blocks(s, (const void *)k_mf_solve, 0);
+    size_t smem = sizeof(MfSolveSmem);
+    cudaFuncSetAttribute(k_mf_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int blocks = mf_blocks(s, (const void *)k_mf_solve, smem);
     if (blocks < 1) {
         s->last_error = "mf_solve: kernel does not fit";
         return EREBUS_ECUDA;
@@ -706,7 +824,7 @@ int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
     void *args[] = {&V, &w, &bar, &err};
     cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
     int rc = check_cuda(s, cudaLaunchCooperativeKernel((const void *)k_mf_solve, blocks,
-                                                       LU_THREADS, args, 0, s->stream),
+                                                       LU_THREADS, args, smem, s->stream),
                         "mf_solve launch");
     s->launches++;
     return rc;
