@@ -250,8 +250,9 @@ def run_ours(args):
     pkg = load_pkg()
     solver = {"multifrontal": 0, "band": 1}[args.direct_solver]
     st = pkg.make_state(args.workload)
+    fp32 = 1 if args.precision == "mixed" else 0
     sim = pkg.Simulation(st)
-    sim.set_solver_options(direct_solver=solver)
+    sim.set_solver_options(direct_solver=solver, factor_fp32=fp32)
     for ts in range(1, args.warmup + 1):
         sim.step(ts)
     sim.enable_phase_timing(True)
@@ -281,7 +282,7 @@ def run_ours(args):
     st2 = pin_host_state(pkg.make_state(args.workload))
     sim.close()
     sim2 = pkg.Simulation(st2)
-    sim2.set_solver_options(direct_solver=solver)
+    sim2.set_solver_options(direct_solver=solver, factor_fp32=fp32)
     for ts in range(1, 3):
         sim2.step(ts)
     sim2.download()
@@ -346,16 +347,21 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if fp32 == 0 else "f64 (factors f32)", "data": "synthetic",
                 "config": config_dict(pkg, args.workload,
                                       {"parallelism": "replicas x%d" % world,
                                        "direct_solver": args.direct_solver,
+                                       "factor_precision": args.precision,
                                        "titer_per_step": [s.titer for s in stats],
                                        "hydro_solves": sum(s.hydro_solves for s in stats),
                                        "thermal_solves": sum(s.thermal_solves for s in stats),
                                        "gravity_solves": sum(s.gravity_solves for s in stats),
                                        "factor_storage_GB": {k: v.storage_bytes / 1e9
-                                                             for k, v in fstats.items()}}),
+                                                             for k, v in fstats.items()},
+                                       "fp64_refactorizations": {
+                                           k: v.fp64_refactorizations
+                                           for k, v in fstats.items()}}),
                 "roofline": roof, "roofline_solve": roof_solve, "phases": per,
                 "cpu_baseline": cpu, "clocks": ck, "e2e": e2e, "gpu_launches": launches}
         print(json.dumps(line), flush=True)
@@ -375,6 +381,8 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=["planetesimal_41", "planetesimal_141", "planetesimal_401"])
     ap.add_argument("--direct-solver", default="multifrontal", choices=["multifrontal", "band"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: FP32 multifrontal factors inside FP64 refinement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -184,10 +184,10 @@ int erebus_default_solver_options(ErebusSolverOptions *o) {
     o->hydro_rtol = 1e-13;
     o->thermal_rtol = 1e-13;
     o->gravity_rtol = 1e-13;
-    o->max_refinements = 4;
+    o->max_refinements = 8;   // refinement stops earlier once a step stops paying
     o->reuse_factors = 1;
     o->direct_solver = EREBUS_SOLVER_MULTIFRONTAL;
-    o->reserved = 0;
+    o->factor_fp32 = 0;
     return EREBUS_OK;
 }
 
@@ -305,6 +305,9 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
     if (band_alloc(s, s->hydro, 6 * (int64_t)np, 6 * g.Ny1 + 2, 64, 12))
         return fail(EREBUS_ENOMEM, "hydro system");
     s->hydro.dofs = 6;
+    s->hydro.name = "Stokes-Darcy";
+    s->thermal.name = "heat";
+    s->gravity.name = "gravity";
     if (band_alloc(s, s->thermal, (int64_t)np, g.Ny1, 64, 5))
         return fail(EREBUS_ENOMEM, "thermal system");
     if (band_alloc(s, s->gravity, (int64_t)np, g.Ny1, 64, 5))
@@ -327,6 +330,7 @@ int erebus_factor_stats(erebus_state *s, int32_t system, ErebusFactorStats *out)
     else band_stats(sys, out);
     out->unknowns = sys.n;
     out->factorizations = sys.factorizations;
+    out->fp64_refactorizations = sys.fp64_refactorizations;
     return EREBUS_OK;
 }
 
@@ -334,7 +338,8 @@ int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o) {
     if (!s || !o) return EREBUS_EINVAL;
     if (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL && o->direct_solver != EREBUS_SOLVER_BAND)
         return EREBUS_EINVAL;
-    if (o->direct_solver != s->opt.direct_solver) {   // factors of the other solver are stale
+    if (o->direct_solver != s->opt.direct_solver ||
+        (o->factor_fp32 != 0) != (s->opt.factor_fp32 != 0)) {   // stale factors
         s->hydro.factored = s->thermal.factored = s->gravity.factored = false;
     }
     s->opt = *o;

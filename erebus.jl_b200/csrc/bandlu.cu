@@ -610,7 +610,7 @@ bool use_multifrontal(const erebus_state *s) {
 }
 
 int band_factor(erebus_state *s, BandSystem &sys) {
-    if (use_multifrontal(s)) return mf_factor(s, sys);
+    if (use_multifrontal(s)) return mf_factor(s, sys, s->opt.factor_fp32 != 0);
     int trc = band_tiles(s, sys);
     if (trc) return trc;
     size_t smem = sizeof(FactorSmem);
@@ -671,6 +671,8 @@ int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir
     if (cold) cudaMemsetAsync(sys.x, 0, np * 8, s->stream);
     double rel = 0.0, prev = INFINITY;
     int solves = 0;
+    bool escalated = false;
+refine:
     double *part = s->norm_part;   // 2 * NORM_BLOCKS partial sums
     for (;;) {
         EREBUS_LAUNCH(s, k_band_residual, nblocks(np), kThreads, 0, B, sys.x, sys.r);
@@ -702,6 +704,25 @@ int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir
         EREBUS_LAUNCH(s, k_axpy, nblocks(np), kThreads, 0, sys.x, sys.d, np);
         solves++;
     }
+    // Mixed precision: when refinement with the FP32 factors stalls above the
+    // target, factor this matrix again in FP64 and go on refining from the
+    // current solution.
+    if (!(rel <= rtol) && !escalated && use_multifrontal(s) && mf_is_fp32(sys)) {
+        escalated = true;
+        timer_end(s, sys.ph_solve);
+        timer_begin(s, sys.ph_factor);
+        rc = mf_factor(s, sys, false);
+        timer_end(s, sys.ph_factor);
+        if (rc) return rc;
+        sys.fp64_refactorizations++;
+        timer_begin(s, sys.ph_solve);
+        prev = INFINITY;
+        if (!(rel < INFINITY)) {
+            cudaMemsetAsync(sys.x, 0, np * 8, s->stream);
+            cold = true;
+        }
+        goto refine;
+    }
     timer_end(s, sys.ph_solve);
     sys.have_x = rel < 1e-6;   // good enough to start the next solve from
     if (st) {
@@ -710,7 +731,11 @@ int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir
         st->rel_residual = rel;
     }
     if (!(rel <= rtol) && !(rel < 1e-6)) {
-        s->last_error = "linear solve did not reach tolerance";
+        char msg[160];
+        snprintf(msg, sizeof msg,
+                 "%s solve did not reach tolerance: relative residual %.3e after %d "
+                 "refinement steps (previous %.3e)", sys.name, rel, solves, prev);
+        s->last_error = msg;
         return EREBUS_ENOCONV;
     }
     return EREBUS_OK;

@@ -26,6 +26,7 @@
 // on the number of CTAs: every tile is computed by one CTA in a fixed order.
 #include <cooperative_groups.h>
 
+#include <type_traits>
 #include <vector>
 
 #include "mf_plan.h"
@@ -39,7 +40,7 @@ static_assert(MF_TILE == NB_TILE, "front tiles are the LU tiles");
 
 struct MfView {
     const MfFront *fr;
-    double *F;          // front storage
+    void *F;            // front storage (double, or float for the mixed-precision factor)
     double *vec;        // front vectors (solve)
     const int *vars;    // local -> global unknown
     const int *eamap;   // local -> children's update index
@@ -54,17 +55,23 @@ struct MfView {
 
 struct MfDevice {
     MfPlan plan;
+    bool fp32 = false;   // the current factors are the float ones
     MfFront *fr = nullptr;
-    double *F = nullptr, *vec = nullptr;
+    void *F64 = nullptr, *F32 = nullptr;   // front storage of each precision, on first use
+    double *vec = nullptr;
     int *vars = nullptr, *eamap = nullptr, *lvl = nullptr, *lvl_kt = nullptr;
     long long *target = nullptr;
     int *expect = nullptr;
     int nlev = 0;
 };
 
-__device__ __forceinline__ double *ftile(const MfView &V, const MfFront &f, int I, int J) {
-    return V.F + f.off + ((long long)J * f.Mt + I) * T2;
+template <class T>
+__device__ __forceinline__ T *ftile(const MfView &V, const MfFront &f, int I, int J) {
+    return (T *)V.F + f.off + ((long long)J * f.Mt + I) * T2;
 }
+// accumulator fragments of a tile product with T-valued tiles
+template <class T> struct MfAccT { typedef double type[2][2][4]; };
+template <> struct MfAccT<float> { typedef float type[2][2][4]; };
 __device__ __forceinline__ long long felem(const MfFront &f, int a, int b) {
     return f.off + ((long long)(b >> 6) * f.Mt + (a >> 6)) * T2 + (b & 63) * 64 + (a & 63);
 }
@@ -72,6 +79,7 @@ __device__ __forceinline__ long long felem(const MfFront &f, int a, int b) {
 // ---------------------------------------------------------------------------
 // assembly
 // ---------------------------------------------------------------------------
+template <class T>
 __global__ void k_mf_scatter(MfView V, const int *cols, const double *vals, int *err) {
     long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= V.n) return;
@@ -83,15 +91,16 @@ __global__ void k_mf_scatter(MfView V, const int *cols, const double *vals, int 
             continue;
         }
         long long t = V.target[e];
-        if (t >= 0) V.F[t] += vals[e];
+        if (t >= 0) ((T *)V.F)[t] += (T)vals[e];
     }
 }
 
+template <class T>
 __global__ void k_mf_pad(MfView V, int nfronts) {
     int f = blockIdx.x;
     if (f >= nfronts) return;
     MfFront fr = V.fr[f];
-    for (int a = fr.k + threadIdx.x; a < fr.Kp; a += blockDim.x) V.F[felem(fr, a, a)] = 1.0;
+    for (int a = fr.k + threadIdx.x; a < fr.Kp; a += blockDim.x) ((T *)V.F)[felem(fr, a, a)] = T(1);
 }
 
 // ---------------------------------------------------------------------------
@@ -102,6 +111,7 @@ __global__ void k_mf_pad(MfView V, int nfronts) {
 // map onto it (child 0 first, then child 1).  The tile's row and column maps
 // are staged in shared memory; a child that maps onto no row or no column
 // of the tile is skipped, and so is the whole tile when neither child does.
+template <class T>
 __device__ void mf_extend_add_tile(const MfView &V, const MfFront &f, int I, int J,
                                    int (*emap)[64]) {
     const int *map = V.eamap + f.map_off;
@@ -119,7 +129,8 @@ __device__ void mf_extend_add_tile(const MfView &V, const MfFront &f, int I, int
     int r1 = __syncthreads_or(which == 1 && any), c1 = __syncthreads_or(which == 3 && any);
     const bool u0 = h0 && r0 && c0, u1 = h1 && r1 && c1;
     if (u0 || u1) {
-        double *T = ftile(V, f, I, J);
+        T *Tt = ftile<T>(V, f, I, J);
+        const T *F = (const T *)V.F;
         MfFront C0, C1;
         if (u0) C0 = V.fr[f.c0];
         if (u1) C1 = V.fr[f.c1];
@@ -127,66 +138,72 @@ __device__ void mf_extend_add_tile(const MfView &V, const MfFront &f, int I, int
         // alias the children's storage as far as the compiler knows)
 #pragma unroll 1
         for (int q0 = 0; q0 < 16; q0 += 8) {
-            double t[8], x0[8], x1[8];
+            T t[8], x0[8], x1[8];
 #pragma unroll
             for (int q = 0; q < 8; q++) {
                 int e = tid + 256 * (q0 + q), r = e & 63, c = e >> 6;
-                t[q] = __ldcg(&T[c * 64 + r]);
-                x0[q] = 0.0;
-                x1[q] = 0.0;
+                t[q] = __ldcg(&Tt[c * 64 + r]);
+                x0[q] = T(0);
+                x1[q] = T(0);
                 if (u0) {
                     int ia = emap[0][r], ib = emap[2][c];
-                    if (ia >= 0 && ib >= 0) x0[q] = __ldcg(V.F + felem(C0, C0.Kp + ia, C0.Kp + ib));
+                    if (ia >= 0 && ib >= 0) x0[q] = __ldcg(F + felem(C0, C0.Kp + ia, C0.Kp + ib));
                 }
                 if (u1) {
                     int ia = emap[1][r], ib = emap[3][c];
-                    if (ia >= 0 && ib >= 0) x1[q] = __ldcg(V.F + felem(C1, C1.Kp + ia, C1.Kp + ib));
+                    if (ia >= 0 && ib >= 0) x1[q] = __ldcg(F + felem(C1, C1.Kp + ia, C1.Kp + ib));
                 }
             }
 #pragma unroll
             for (int q = 0; q < 8; q++) {
                 int e = tid + 256 * (q0 + q), r = e & 63, c = e >> 6;
-                T[c * 64 + r] = (t[q] + x0[q]) + x1[q];
+                Tt[c * 64 + r] = (t[q] + x0[q]) + x1[q];
             }
         }
     }
     __syncthreads();
 }
 
-// Inverts tile T in place (Gauss-Jordan in the FFMA register layout).
-__device__ void mf_invert_tile(double *T, MmaSmem &S, int *err) {
+// Inverts tile T in place (Gauss-Jordan in FP64 registers, FFMA layout).
+template <class T>
+__device__ void mf_invert_tile(T *Tt, MmaSmem &S, int *err) {
     double a[4][4];
     double *P = S.stage[0];
-    stage_tile(P, T);
+    stage_tile(P, Tt);
     __syncthreads();
     regs_from_smem(P, a);
     __syncthreads();
     tile_inverse2(a, S.vec, err);
     regs_to_smem(P, a);
     __syncthreads();
-    unstage_tile(T, P);
+    unstage_tile(Tt, P);
     __syncthreads();
 }
 
 // L_IK = A_IK D_K^{-1} (tile (K,K) holds D_K^{-1})
+template <class T>
 __device__ void mf_l_tile(const MfView &V, const MfFront &f, int I, int K, MmaSmem &S) {
-    MmaAcc acc;
-    const double *A = ftile(V, f, I, K), *B = ftile(V, f, K, K);
+    typename MfAccT<T>::type acc;
+    typedef typename std::remove_reference<decltype(acc[0][0][0])>::type A;
+    const T *At = ftile<T>(V, f, I, K), *Bt = ftile<T>(V, f, K, K);
     mma_tiles(
-        S, 1, [&](int) { return A; }, [&](int) { return B; }, acc, [&] { frag_zero(acc); });
-    frag_store(ftile(V, f, I, K), acc, 1.0);
+        S, 1, [&](int) { return At; }, [&](int) { return Bt; }, acc, [&] { frag_zero(acc); });
+    frag_store(ftile<T>(V, f, I, K), acc, A(1));
     __syncthreads();
 }
 
 // A_IJ -= sum_{K in [k0, k1)} L_IK A_KJ; optionally invert the result.
+template <class T>
 __device__ void mf_update_tile(const MfView &V, const MfFront &f, int I, int J, int k0,
                                int k1, MmaSmem &S, int *err, bool invert) {
-    MmaAcc acc;
-    double *C = ftile(V, f, I, J);
+    typedef typename MfAccT<T>::type Acc;
+    Acc acc;
+    typedef typename std::remove_reference<decltype(acc[0][0][0])>::type A;
+    T *C = ftile<T>(V, f, I, J);
     mma_tiles(
-        S, k1 - k0, [&](int p) { return (const double *)ftile(V, f, I, k0 + p); },
-        [&](int p) { return (const double *)ftile(V, f, k0 + p, J); }, acc,
-        [&] { frag_load(C, acc, -1.0); });
+        S, k1 - k0, [&](int p) { return (const T *)ftile<T>(V, f, I, k0 + p); },
+        [&](int p) { return (const T *)ftile<T>(V, f, k0 + p, J); }, acc,
+        [&] { frag_load(C, acc, A(-1)); });
     if (invert) {
         double a[4][4];
         double *P = S.stage[0];
@@ -199,7 +216,7 @@ __device__ void mf_update_tile(const MfView &V, const MfFront &f, int I, int J, 
         __syncthreads();
         unstage_tile(C, P);
     } else {
-        frag_store(C, acc, -1.0);
+        frag_store(C, acc, A(-1));
     }
     __syncthreads();
 }
@@ -235,27 +252,28 @@ __device__ __forceinline__ void mf_upd_ij(const MfFront &f, int K, int u, int &I
 }
 
 // The whole partial LU of one front by one CTA.
+template <class T>
 __device__ void mf_factor_local(const MfView &V, const MfFront &f, MfFactorSmem &FS,
                                 int *err) {
     MmaSmem &S = FS.m;
     if (f.c0 >= 0 || f.c1 >= 0) {
         for (int t = 0; t < f.Mt * f.Mt; t++)
-            mf_extend_add_tile(V, f, t % f.Mt, t / f.Mt, FS.emap);
+            mf_extend_add_tile<T>(V, f, t % f.Mt, t / f.Mt, FS.emap);
         __threadfence_block();
         __syncthreads();
     }
     for (int K = 0; K < f.Kt; K++) {
-        if (K == 0) mf_invert_tile(ftile(V, f, 0, 0), S, err);
-        for (int I = K + 1; I < f.Mt; I++) mf_l_tile(V, f, I, K, S);
+        if (K == 0) mf_invert_tile(ftile<T>(V, f, 0, 0), S, err);
+        for (int I = K + 1; I < f.Mt; I++) mf_l_tile<T>(V, f, I, K, S);
         int nu = mf_nupd(f.Kt, f.Mt, K);
         for (int u = 0; u < nu; u++) {
             int I, J;
             mf_upd_ij(f, K, u, I, J);
-            mf_update_tile(V, f, I, J, K, K + 1, S, err, I == K + 1 && J == K + 1);
+            mf_update_tile<T>(V, f, I, J, K, K + 1, S, err, I == K + 1 && J == K + 1);
         }
     }
     for (int J = f.Kt; J < f.Mt; J++)
-        for (int I = f.Kt; I < f.Mt; I++) mf_update_tile(V, f, I, J, 0, f.Kt, S, err, false);
+        for (int I = f.Kt; I < f.Mt; I++) mf_update_tile<T>(V, f, I, J, 0, f.Kt, S, err, false);
 }
 
 // Runs task(f, u) for the tasks u in [0, count(Kt, Mt)) of the fronts
@@ -289,6 +307,7 @@ __device__ __forceinline__ void mf_load_km(const MfView &V, int fb, int fe, int2
     __syncthreads();
 }
 
+template <class T>
 __global__ void __launch_bounds__(LU_THREADS, 2)
 k_mf_factor(MfView V, unsigned int *bar, int *err) {
     extern __shared__ __align__(16) double smem_raw[];
@@ -300,7 +319,7 @@ k_mf_factor(MfView V, unsigned int *bar, int *err) {
         if (fe - fb >= G / 2 || fe - fb > MF_KM_MAX) {
             for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
                 const MfFront f = V.fr[fi];
-                mf_factor_local(V, f, FS, err);
+                mf_factor_local<T>(V, f, FS, err);
             }
             grid_barrier(bar, err);
             continue;
@@ -311,22 +330,22 @@ k_mf_factor(MfView V, unsigned int *bar, int *err) {
             V, fb, fe, FS.km, [](int, int Mt) { return Mt * Mt; },
             [&](const MfFront &f, int u) {
                 int I = u % f.Mt, J = u / f.Mt;
-                if (f.c0 >= 0 || f.c1 >= 0) mf_extend_add_tile(V, f, I, J, FS.emap);
-                if (u == 0 && f.Kt > 0) mf_invert_tile(ftile(V, f, 0, 0), S, err);
+                if (f.c0 >= 0 || f.c1 >= 0) mf_extend_add_tile<T>(V, f, I, J, FS.emap);
+                if (u == 0 && f.Kt > 0) mf_invert_tile(ftile<T>(V, f, 0, 0), S, err);
             });
         grid_barrier(bar, err);
         const int ktmax = V.lvl_kt[p];
         for (int K = 0; K < ktmax; K++) {
             mf_for_tasks(
                 V, fb, fe, FS.km, [K](int Kt, int Mt) { return K < Kt ? Mt - K - 1 : 0; },
-                [&](const MfFront &f, int u) { mf_l_tile(V, f, K + 1 + u, K, S); });
+                [&](const MfFront &f, int u) { mf_l_tile<T>(V, f, K + 1 + u, K, S); });
             grid_barrier(bar, err);
             mf_for_tasks(
                 V, fb, fe, FS.km, [K](int Kt, int Mt) { return mf_nupd(Kt, Mt, K); },
                 [&](const MfFront &f, int u) {
                     int I, J;
                     mf_upd_ij(f, K, u, I, J);
-                    mf_update_tile(V, f, I, J, K, K + 1, S, err, I == K + 1 && J == K + 1);
+                    mf_update_tile<T>(V, f, I, J, K, K + 1, S, err, I == K + 1 && J == K + 1);
                 });
             grid_barrier(bar, err);
         }
@@ -334,7 +353,7 @@ k_mf_factor(MfView V, unsigned int *bar, int *err) {
             V, fb, fe, FS.km, [](int Kt, int Mt) { return (Mt - Kt) * (Mt - Kt); },
             [&](const MfFront &f, int u) {
                 int ru = f.Mt - f.Kt;
-                mf_update_tile(V, f, f.Kt + u % ru, f.Kt + u / ru, 0, f.Kt, S, err, false);
+                mf_update_tile<T>(V, f, f.Kt + u % ru, f.Kt + u / ru, 0, f.Kt, S, err, false);
             });
         grid_barrier(bar, err);
     }
@@ -363,16 +382,17 @@ __device__ __forceinline__ uint32_t mf_smem(const void *p) {
 }
 
 // Issues the copy of one 64 x 64 tile into slot `sl` (thread 0).
-__device__ __forceinline__ void mf_fetch(MfSolveSmem &S, int sl, const double *src) {
+template <class T>
+__device__ __forceinline__ void mf_fetch(MfSolveSmem &S, int sl, const T *src) {
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
                          mf_smem(&S.bar[sl])),
-                     "r"((uint32_t)(T2 * sizeof(double)))
+                     "r"((uint32_t)(T2 * sizeof(T)))
                      : "memory");
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
             "[%3];" ::"r"(mf_smem(S.tile[sl])),
-            "l"(src), "r"((uint32_t)(T2 * sizeof(double))), "r"(mf_smem(&S.bar[sl]))
+            "l"(src), "r"((uint32_t)(T2 * sizeof(T))), "r"(mf_smem(&S.bar[sl]))
             : "memory");
     }
 }
@@ -407,7 +427,7 @@ __device__ void mf_stream(MfSolveSmem &S, uint32_t *uses, int n, Src src, Use us
         const int sl = i % MF_SLOTS;
         mf_slot_wait(S, sl, uses[sl] & 1u, err);
         uses[sl]++;
-        use(i, S.tile[sl]);
+        use(i, (const decltype(src(0)))S.tile[sl]);
         __syncthreads();
         if (i + MF_SLOTS < n) mf_fetch(S, sl, src(i + MF_SLOTS));
     }
@@ -415,15 +435,16 @@ __device__ void mf_stream(MfSolveSmem &S, uint32_t *uses, int n, Src src, Use us
 
 // Thread (r, q) = (tid % 64, tid / 64): its share of row r of T x, columns
 // 16 q .. 16 q + 15 (T in shared memory, column-major; x in shared memory).
-__device__ __forceinline__ double mf_quarter(const double *T, const double *x) {
+template <class T>
+__device__ __forceinline__ double mf_quarter(const T *Tt, const double *x) {
     const int r = threadIdx.x & 63, q = threadIdx.x >> 6;
-    const double *t = T + q * 16 * 64 + r;
+    const T *t = Tt + q * 16 * 64 + r;
     const double *xx = x + q * 16;
     double s0 = 0.0, s1 = 0.0;
 #pragma unroll
     for (int c = 0; c < 16; c += 2) {
-        s0 = fma(t[c * 64], xx[c], s0);
-        s1 = fma(t[(c + 1) * 64], xx[c + 1], s1);
+        s0 = fma((double)t[c * 64], xx[c], s0);
+        s1 = fma((double)t[(c + 1) * 64], xx[c + 1], s1);
     }
     return s0 + s1;
 }
@@ -469,6 +490,7 @@ __device__ void mf_gather_fwd(const MfView &V, const MfFront &f, const double *w
 // Forward elimination inside a front: for each block column K < Kt, rows
 // I in (K, iend) get v_I -= L_IK y_K, with y_K = v_K final once column K
 // starts.  The tiles stream in column order.
+template <class T>
 __device__ void mf_fwd_front(const MfView &V, const MfFront &f, double *v, int iend,
                              MfSolveSmem &S, uint32_t *uses, int *err) {
     // tile i -> (K, I): columns K = 0.. with iend - K - 1 tiles each
@@ -481,13 +503,13 @@ __device__ void mf_fwd_front(const MfView &V, const MfFront &f, double *v, int i
             fk++;
             fi = fk + 1;
         }
-        const double *t = ftile(V, f, fi, fk);
+        const T *t = ftile<T>(V, f, fi, fk);
         fi++;
         return t;
     };
     mf_stream(
         S, uses, n, src,
-        [&](int, const double *T) {
+        [&](int, const T *Tt) {
             while (I >= iend) {
                 K++;
                 I = K + 1;
@@ -496,7 +518,7 @@ __device__ void mf_fwd_front(const MfView &V, const MfFront &f, double *v, int i
                 if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
                 __syncthreads();
             }
-            double t = mf_reduce_rows(S, mf_quarter(T, S.y));
+            double t = mf_reduce_rows(S, mf_quarter(Tt, S.y));
             if (threadIdx.x < 64) {
                 double *d = &v[I * 64 + threadIdx.x];
                 __stcg(d, __ldcg(d) - t);
@@ -508,16 +530,16 @@ __device__ void mf_fwd_front(const MfView &V, const MfFront &f, double *v, int i
 
 // v_I -= sum_{K in [k0, k1)} T(I, K) x_K for one tile row I; xsrc(K, c)
 // gives element c of the vector piece K.
-template <class Xsrc>
+template <class T, class Xsrc>
 __device__ void mf_row_gemv(const MfView &V, const MfFront &f, double *v, int I, int k0, int k1,
                             Xsrc xsrc, MfSolveSmem &S, uint32_t *uses, int *err) {
     double acc = 0.0;
     mf_stream(
-        S, uses, k1 - k0, [&](int i) { return (const double *)ftile(V, f, I, k0 + i); },
-        [&](int i, const double *T) {
+        S, uses, k1 - k0, [&](int i) { return (const T *)ftile<T>(V, f, I, k0 + i); },
+        [&](int i, const T *Tt) {
             if (threadIdx.x < 64) S.x[threadIdx.x] = xsrc(k0 + i, threadIdx.x);
             __syncthreads();
-            acc += mf_quarter(T, S.x);
+            acc += mf_quarter(Tt, S.x);
         },
         err);
     double t = mf_reduce_rows(S, acc);
@@ -532,6 +554,7 @@ __device__ void mf_row_gemv(const MfView &V, const MfFront &f, double *v, int I,
 // subtracted): for K = Kt-1 .. 0, x_K = D_K^{-1} v_K, then v_I -= U_IK x_K
 // for I < K.  The solution goes to v and to w.  Tiles stream as (K,K),
 // (0,K), (1,K), ..., (K-1,K) for K descending.
+template <class T>
 __device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, double *wout,
                              MfSolveSmem &S, uint32_t *uses, int *err) {
     const int *var = V.vars + f.var_off;
@@ -543,13 +566,13 @@ __device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, doubl
             fk--;
             fj = 0;
         }
-        const double *t = fj == 0 ? ftile(V, f, fk, fk) : ftile(V, f, fj - 1, fk);
+        const T *t = fj == 0 ? ftile<T>(V, f, fk, fk) : ftile<T>(V, f, fj - 1, fk);
         fj++;
         return t;
     };
     mf_stream(
         S, uses, n, src,
-        [&](int, const double *T) {
+        [&](int, const T *Tt) {
             if (j > K) {
                 K--;
                 j = 0;
@@ -557,7 +580,7 @@ __device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, doubl
             if (j == 0) {   // x_K = D_K^{-1} v_K
                 if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
                 __syncthreads();
-                double x = mf_reduce_rows(S, mf_quarter(T, S.y));
+                double x = mf_reduce_rows(S, mf_quarter(Tt, S.y));
                 if (threadIdx.x < 64) {
                     const int r = threadIdx.x, a = K * 64 + r;
                     S.x[r] = x;
@@ -566,7 +589,7 @@ __device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, doubl
                 }
                 __syncthreads();
             } else {        // v_I -= U_IK x_K, I = j - 1
-                double t = mf_reduce_rows(S, mf_quarter(T, S.x));
+                double t = mf_reduce_rows(S, mf_quarter(Tt, S.x));
                 if (threadIdx.x < 64) {
                     double *d = &v[(j - 1) * 64 + threadIdx.x];
                     __stcg(d, __ldcg(d) - t);
@@ -578,6 +601,7 @@ __device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, doubl
 }
 
 // Solves L U x = w in place (w: n values; rows >= n untouched).
+template <class T>
 __global__ void __launch_bounds__(LU_THREADS, 2)
 k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
     extern __shared__ __align__(128) double smem_raw[];
@@ -602,7 +626,7 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
             const MfFront f = V.fr[fi];
             double *v = V.vec + f.vec_off;
             mf_gather_fwd(V, f, w, v);
-            mf_fwd_front(V, f, v, local ? f.Mt : f.Kt, S, uses, err);
+            mf_fwd_front<T>(V, f, v, local ? f.Mt : f.Kt, S, uses, err);
         }
         if (!local) {
             grid_barrier(bar, err);
@@ -611,7 +635,7 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
                 V, fb, fe, S.km, [](int Kt, int Mt) { return Mt - Kt; },
                 [&](const MfFront &f, int u) {
                     double *v = V.vec + f.vec_off;
-                    mf_row_gemv(
+                    mf_row_gemv<T>(
                         V, f, v, f.Kt + u, 0, f.Kt,
                         [&](int K, int c) { return __ldcg(&v[K * 64 + c]); }, S, uses, err);
                 });
@@ -635,8 +659,8 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
             mf_for_tasks(
                 V, fb, fe, S.km, [](int Kt, int Mt) { return Mt > Kt ? Kt : 0; },
                 [&](const MfFront &f, int u) {
-                    mf_row_gemv(V, f, V.vec + f.vec_off, u, f.Kt, f.Mt, ring_x(f), S, uses,
-                                err);
+                    mf_row_gemv<T>(V, f, V.vec + f.vec_off, u, f.Kt, f.Mt, ring_x(f), S, uses,
+                                   err);
                 });
             grid_barrier(bar, err);
         }
@@ -645,8 +669,8 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
             double *v = V.vec + f.vec_off;
             if (local)
                 for (int K = 0; K < f.Kt && f.Mt > f.Kt; K++)
-                    mf_row_gemv(V, f, v, K, f.Kt, f.Mt, ring_x(f), S, uses, err);
-            mf_bwd_front(V, f, v, w, S, uses, err);
+                    mf_row_gemv<T>(V, f, v, K, f.Kt, f.Mt, ring_x(f), S, uses, err);
+            mf_bwd_front<T>(V, f, v, w, S, uses, err);
         }
         grid_barrier(bar, err);
     }
@@ -658,7 +682,7 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
 static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
     MfView V;
     V.fr = D.fr;
-    V.F = D.F;
+    V.F = D.fp32 ? D.F32 : D.F64;
     V.vec = D.vec;
     V.vars = D.vars;
     V.eamap = D.eamap;
@@ -672,10 +696,12 @@ static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
     return V;
 }
 
+bool mf_is_fp32(const BandSystem &sys) { return sys.mf && sys.mf->fp32; }
+
 void mf_release(BandSystem &sys) {
     MfDevice *D = sys.mf;
     if (!D) return;
-    void *ps[] = {D->fr, D->F, D->vec, D->vars, D->eamap, D->lvl, D->lvl_kt, D->target,
+    void *ps[] = {D->fr, D->F64, D->F32, D->vec, D->vars, D->eamap, D->lvl, D->lvl_kt, D->target,
                   D->expect};
     for (void *p : ps)
         if (p) cudaFree(p);
@@ -733,7 +759,6 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
     if (e == cudaSuccess) e = upload(&D->lvl_kt, lvl_kt, s->stream);
     if (e == cudaSuccess) e = upload(&D->target, target, s->stream);
     if (e == cudaSuccess) e = upload(&D->expect, expect, s->stream);
-    if (e == cudaSuccess) e = cudaMalloc(&D->F, P.storage * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&D->vec, P.vec * sizeof(double));
     if (e != cudaSuccess) {
         s->last_error = std::string("multifrontal allocation: ") + cudaGetErrorString(e);
@@ -749,24 +774,31 @@ static int mf_blocks(erebus_state *s, const void *func, size_t smem) {
     return std::min(per_sm, 2) * sms;
 }
 
-int mf_factor(erebus_state *s, BandSystem &sys) {
-    int rc;
-    if (!sys.mf) {
-        rc = mf_prepare(s, sys, sys.dofs);
-        if (rc) return rc;
-    }
+template <class T>
+static int mf_factor_t(erebus_state *s, BandSystem &sys) {
     MfDevice &D = *sys.mf;
+    void *&F = sizeof(T) == 4 ? D.F32 : D.F64;
+    if (!F) {
+        cudaError_t e = cudaMalloc(&F, D.plan.storage * sizeof(T));
+        if (e != cudaSuccess) {
+            F = nullptr;
+            s->last_error = std::string("multifrontal factor storage: ") + cudaGetErrorString(e);
+            return EREBUS_ENOMEM;
+        }
+    }
+    D.fp32 = sizeof(T) == 4;
     MfView V = mf_view(D, sys);
-    rc = check_cuda(s, cudaMemsetAsync(D.F, 0, D.plan.storage * sizeof(double), s->stream),
-                    "mf zero");
+    int rc = check_cuda(s, cudaMemsetAsync(F, 0, D.plan.storage * sizeof(T), s->stream),
+                        "mf zero");
     if (rc) return rc;
-    EREBUS_LAUNCH(s, k_mf_scatter, nblocks(sys.n), kThreads, 0, V, sys.ell_cols, sys.ell_vals,
-                  sys.err);
+    EREBUS_LAUNCH(s, k_mf_scatter<T>, nblocks(sys.n), kThreads, 0, V, sys.ell_cols,
+                  sys.ell_vals, sys.err);
     int nf = (int)D.plan.fronts.size();
-    EREBUS_LAUNCH(s, k_mf_pad, nf, 64, 0, V, nf);
+    EREBUS_LAUNCH(s, k_mf_pad<T>, nf, 64, 0, V, nf);
     size_t smem = sizeof(MfFactorSmem);
-    cudaFuncSetAttribute(k_mf_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int blocks = mf_blocks(s, (const void *)k_mf_factor, smem);
+    const void *fn = (const void *)k_mf_factor<T>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int blocks = mf_blocks(s, fn, smem);
     if (blocks < 1) {
         s->last_error = "mf_factor: kernel does not fit";
         return EREBUS_ECUDA;
@@ -775,10 +807,20 @@ int mf_factor(erebus_state *s, BandSystem &sys) {
     int *err = sys.err;
     void *args[] = {&V, &bar, &err};
     cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
-    rc = check_cuda(s, cudaLaunchCooperativeKernel((const void *)k_mf_factor, blocks,
-                                                   LU_THREADS, args, smem, s->stream),
+    rc = check_cuda(s, cudaLaunchCooperativeKernel(fn, blocks, LU_THREADS, args, smem,
+                                                   s->stream),
                     "mf_factor launch");
     s->launches++;
+    return rc;
+}
+
+int mf_factor(erebus_state *s, BandSystem &sys, bool fp32) {
+    int rc;
+    if (!sys.mf) {
+        rc = mf_prepare(s, sys, sys.dofs);
+        if (rc) return rc;
+    }
+    rc = fp32 ? mf_factor_t<float>(s, sys) : mf_factor_t<double>(s, sys);
     if (rc) return rc;
     sys.factored = true;
     sys.factorizations++;
@@ -800,9 +842,10 @@ void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o
     }
     o->fronts = (int32_t)P.fronts.size();
     o->levels = (int32_t)P.level_begin.size() - 1;
-    o->storage_bytes = P.storage * (int64_t)sizeof(double);
+    const int es = s->opt.factor_fp32 ? sizeof(float) : sizeof(double);
+    o->storage_bytes = P.storage * (int64_t)es;
     o->flops = tiles * 2.0 * T2 * NB_TILE;
-    o->solve_bytes = rd * T2 * sizeof(double);
+    o->solve_bytes = rd * T2 * es;
 }
 
 int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
@@ -813,8 +856,9 @@ int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
     MfDevice &D = *sys.mf;
     MfView V = mf_view(D, sys);
     size_t smem = sizeof(MfSolveSmem);
-    cudaFuncSetAttribute(k_mf_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int blocks = mf_blocks(s, (const void *)k_mf_solve, smem);
+    const void *fn = D.fp32 ? (const void *)k_mf_solve<float> : (const void *)k_mf_solve<double>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int blocks = mf_blocks(s, fn, smem);
     if (blocks < 1) {
         s->last_error = "mf_solve: kernel does not fit";
         return EREBUS_ECUDA;
@@ -823,8 +867,8 @@ int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
     int *err = sys.err;
     void *args[] = {&V, &w, &bar, &err};
     cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
-    int rc = check_cuda(s, cudaLaunchCooperativeKernel((const void *)k_mf_solve, blocks,
-                                                       LU_THREADS, args, smem, s->stream),
+    int rc = check_cuda(s, cudaLaunchCooperativeKernel(fn, blocks, LU_THREADS, args, smem,
+                                                       s->stream),
                         "mf_solve launch");
     s->launches++;
     return rc;

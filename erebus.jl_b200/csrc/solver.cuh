@@ -54,7 +54,8 @@ int band_apply_unscaled(erebus_state *s, BandSystem &sys, const double *x, doubl
 int assemble_system(erebus_state *s, int kind);
 // Nested-dissection multifrontal LU (mfront.cu): factor the assembled ELL
 // matrix of `sys`, solve in place, release the factor storage.
-int mf_factor(erebus_state *s, BandSystem &sys);
+int mf_factor(erebus_state *s, BandSystem &sys, bool fp32);
+bool mf_is_fp32(const BandSystem &sys);
 int mf_solve(erebus_state *s, BandSystem &sys, double *w);
 void mf_release(BandSystem &sys);
 void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o);

@@ -67,6 +67,7 @@ struct MfDevice;   // multifrontal factor storage and plan (mfront.cu)
 struct BandSystem {
     int64_t n = 0;             // unknowns
     int dofs = 1;              // unknowns per P node
+    const char *name = "";     // for error messages
     int b = 0;                 // half bandwidth (max |row-col|)
     int nb = 0;                // tile size
     int NB = 0;                // tile rows/cols
@@ -88,6 +89,7 @@ struct BandSystem {
     bool factored = false;
     bool have_x = false;           // x holds a converged solution
     int factorizations = 0;        // number of factorisations so far
+    int fp64_refactorizations = 0; // FP64 factorisations after stalled FP32 refinement
     int ph_factor = -1, ph_solve = -1;   // timer phases of this system
 };
 

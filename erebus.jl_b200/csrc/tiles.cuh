@@ -373,42 +373,168 @@ static __device__ __forceinline__ int frag_col(int ni, int q) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     return (w >> 1) * 16 + ni * 8 + 2 * (lane & 3) + (q & 1);
 }
-static __device__ __forceinline__ void frag_zero(MmaAcc acc) {
+template <class A>
+static __device__ __forceinline__ void frag_zero(A acc[2][2][4]) {
 #pragma unroll
     for (int mi = 0; mi < 2; mi++)
 #pragma unroll
         for (int ni = 0; ni < 2; ni++)
 #pragma unroll
-            for (int q = 0; q < 4; q++) acc[mi][ni][q] = 0.0;
+            for (int q = 0; q < 4; q++) acc[mi][ni][q] = A(0);
 }
 // acc = sign * C (global column-major tile, read through L2)
-static __device__ __forceinline__ void frag_load(const double *C, MmaAcc acc, double sign) {
+template <class T, class A>
+static __device__ __forceinline__ void frag_load(const T *C, A acc[2][2][4], A sign) {
 #pragma unroll
     for (int mi = 0; mi < 2; mi++)
 #pragma unroll
         for (int ni = 0; ni < 2; ni++)
 #pragma unroll
             for (int q = 0; q < 4; q++)
-                acc[mi][ni][q] = sign * __ldcg(&C[frag_col(ni, q) * NB_TILE + frag_row(mi, q)]);
+                acc[mi][ni][q] = sign * (A)__ldcg(&C[frag_col(ni, q) * NB_TILE + frag_row(mi, q)]);
 }
-static __device__ __forceinline__ void frag_store(double *C, const MmaAcc acc, double sign) {
+template <class T, class A>
+static __device__ __forceinline__ void frag_store(T *C, const A acc[2][2][4], A sign) {
 #pragma unroll
     for (int mi = 0; mi < 2; mi++)
 #pragma unroll
         for (int ni = 0; ni < 2; ni++)
 #pragma unroll
             for (int q = 0; q < 4; q++)
-                C[frag_col(ni, q) * NB_TILE + frag_row(mi, q)] = sign * acc[mi][ni][q];
+                C[frag_col(ni, q) * NB_TILE + frag_row(mi, q)] = (T)(sign * acc[mi][ni][q]);
 }
-// fragments -> shared-memory tile (column-major, ld LDS)
-static __device__ __forceinline__ void frag_to_smem(double *T, const MmaAcc acc, double sign) {
+// fragments -> shared-memory FP64 tile (column-major, ld LDS)
+template <class A>
+static __device__ __forceinline__ void frag_to_smem(double *T, const A acc[2][2][4], double sign) {
 #pragma unroll
     for (int mi = 0; mi < 2; mi++)
 #pragma unroll
         for (int ni = 0; ni < 2; ni++)
 #pragma unroll
             for (int q = 0; q < 4; q++)
-                T[frag_col(ni, q) * LDS + frag_row(mi, q)] = sign * acc[mi][ni][q];
+                T[frag_col(ni, q) * LDS + frag_row(mi, q)] = sign * (double)acc[mi][ni][q];
+}
+
+// ---------------------------------------------------------------------------
+// FP32 tiles (mixed-precision factor): 64 x 64 float tiles, products on the
+// tensor cores with three TF32 products per FP32 product (x = hi + lo with
+// hi, lo TF32; a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi), which keeps about
+// FP32 accuracy; accumulation in FP32.  A stage holds a whole tile pair:
+// A column-major with leading dimension 72, B column-major with leading
+// dimension 68 (fragment loads hit every bank once); the same bytes as an
+// FP64 stage.
+// ---------------------------------------------------------------------------
+constexpr int MMAF_LA = 72, MMAF_LB = 68;
+static_assert((NB_TILE * MMAF_LA + NB_TILE * MMAF_LB) * 4 <= MMA_STAGE * 8, "float stage fits");
+typedef float MmaAccF[2][2][4];
+
+static __device__ __forceinline__ void mma_load_pair_f(float *st, const float *A, const float *B) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int e = threadIdx.x + 256 * q;
+        int col = e >> 4, rq = (e & 15) * 4;
+        cp_async16(st + col * MMAF_LA + rq, A + col * NB_TILE + rq);
+    }
+    float *sb = st + NB_TILE * MMAF_LA;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int e = threadIdx.x + 256 * q;
+        int c = e >> 4, kq = (e & 15) * 4;
+        cp_async16(sb + c * MMAF_LB + kq, B + c * NB_TILE + kq);
+    }
+}
+
+static __device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) {
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+    float r = x - __uint_as_float(hi);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+static __device__ __forceinline__ void mma_tf32(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// acc += (pair's A) * (pair's B), K = 64 in steps of 8
+static __device__ __forceinline__ void mma_pair_f(const float *st, MmaAccF acc) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int rb = (w & 1) * 32, cb = (w >> 1) * 16;
+    const float *sa = st, *sb = st + NB_TILE * MMAF_LA;
+#pragma unroll 2
+    for (int ks = 0; ks < NB_TILE; ks += 8) {
+        uint32_t ah[2][4], al[2][4], bh[2][2], bl[2][2];
+#pragma unroll
+        for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                tf32_split(sa[(ks + t + 4 * (i >> 1)) * MMAF_LA + rb + mi * 16 + g + 8 * (i & 1)],
+                           ah[mi][i], al[mi][i]);
+#pragma unroll
+        for (int ni = 0; ni < 2; ni++)
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+                tf32_split(sb[(cb + ni * 8 + g) * MMAF_LB + ks + t + 4 * i], bh[ni][i], bl[ni][i]);
+#pragma unroll
+        for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+            for (int ni = 0; ni < 2; ni++) {
+                mma_tf32(acc[mi][ni], al[mi], bh[ni]);
+                mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
+                mma_tf32(acc[mi][ni], ah[mi], bh[ni]);
+            }
+    }
+}
+
+// acc += sum_{p < np} tileA(p) * tileB(p) for float tiles; three-stage
+// cp.async pipeline over the tile pairs; `pre()` as in mma_tiles.
+template <class TA, class TB, class Pre>
+static __device__ void mma_tiles(MmaSmem &S, int np, TA tileA, TB tileB, MmaAccF acc, Pre pre) {
+#pragma unroll 1
+    for (int q = 0; q < 2; q++) {
+        if (q < np) mma_load_pair_f(reinterpret_cast<float *>(S.stage[q]), tileA(q), tileB(q));
+        cp_async_commit();
+    }
+    pre();
+#pragma unroll 1
+    for (int q = 0; q < np; q++) {
+        cp_async_wait1();
+        __syncthreads();
+        if (q + 2 < np)
+            mma_load_pair_f(reinterpret_cast<float *>(S.stage[(q + 2) % MMA_NSTAGE]),
+                            tileA(q + 2), tileB(q + 2));
+        cp_async_commit();
+        mma_pair_f(reinterpret_cast<const float *>(S.stage[q % MMA_NSTAGE]), acc);
+    }
+    cp_async_wait0();
+    __syncthreads();
+}
+
+// float tile (global, column-major) <-> FP64 shared-memory tile (ld LDS)
+static __device__ __forceinline__ void stage_tile(double *dst, const float *src) {
+    const float4 *s4 = reinterpret_cast<const float4 *>(src);
+    float4 v[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) v[q] = __ldcg(&s4[threadIdx.x + 256 * q]);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int e = 4 * (threadIdx.x + 256 * q), r = e % NB_TILE, c = e / NB_TILE;
+        dst[c * LDS + r] = v[q].x;
+        dst[c * LDS + r + 1] = v[q].y;
+        dst[c * LDS + r + 2] = v[q].z;
+        dst[c * LDS + r + 3] = v[q].w;
+    }
+}
+static __device__ __forceinline__ void unstage_tile(float *dst, const double *src) {
+    float4 *d4 = reinterpret_cast<float4 *>(dst);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int e = 4 * (threadIdx.x + 256 * q), r = e % NB_TILE, c = e / NB_TILE;
+        d4[threadIdx.x + 256 * q] =
+            make_float4((float)src[c * LDS + r], (float)src[c * LDS + r + 1],
+                        (float)src[c * LDS + r + 2], (float)src[c * LDS + r + 3]);
+    }
 }
 
 }  // namespace erebus

@@ -183,7 +183,10 @@ typedef struct ErebusSolverOptions {
     int32_t reuse_factors;     /* 1: keep the LU factors while the scaled
                                   matrix is bitwise unchanged */
     int32_t direct_solver;     /* EREBUS_SOLVER_MULTIFRONTAL or EREBUS_SOLVER_BAND */
-    int32_t reserved;
+    int32_t factor_fp32;       /* 1: mixed precision -- the multifrontal factors are
+                                  computed and stored in FP32 (tensor-core products
+                                  with three TF32 terms), residuals and refinement
+                                  stay FP64 */
 } ErebusSolverOptions;
 
 /* Size and work of one system's direct solver (diagnostics; no reference
@@ -198,6 +201,10 @@ typedef struct ErebusFactorStats {
     int32_t fronts;            /* multifrontal fronts (0 for the band LU) */
     int32_t levels;            /* tree levels (band LU: tile rows) */
     int32_t factorizations;    /* factorisations so far */
+    int32_t fp64_refactorizations; /* mixed precision: matrices factored again in
+                                      FP64 because refinement with the FP32
+                                      factors stalled */
+    int32_t reserved;
     int64_t unknowns;
     int64_t storage_bytes;     /* factor storage */
     double  flops;             /* per factorisation */

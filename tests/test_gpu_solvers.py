@@ -1,5 +1,5 @@
-"""GPU: the two direct solvers of the library against each other and
-against the oracle.
+"""GPU: the direct solvers of the library against each other and against
+the oracle.
 
 The default solver is the nested-dissection multifrontal LU; the
 block-banded LU in the reference's unknown order is the alternative
@@ -30,10 +30,10 @@ def state41(pkg, oracle):
     return st
 
 
-def _hydro_pass(pkg, st, solver):
+def _hydro_pass(pkg, st, solver, fp32=0):
     s = st.copy()
     sim = pkg.Simulation(s)
-    sim.set_solver_options(direct_solver=solver)
+    sim.set_solver_options(direct_solver=solver, factor_fp32=fp32)
     sim.markers_to_nodes(s.timesum)
     sim.gravity()
     dt, conv, stats = sim.hydromech_pass(s.dt, 1)
@@ -71,6 +71,48 @@ def test_multifrontal_steps_141(pkg, built_lib):
         sim.close()
         out[solver] = st
     a, b = out[0], out[1]
+    assert a.marknum == b.marknum
+    n = a.marknum
+    for k in ("xm", "ym"):
+        d = np.max(np.abs(a.m[k][:n] - b.m[k][:n])) / np.max(np.abs(b.m[k][:n]))
+        assert d < 1e-10, (k, d)
+    for k in ("tk2", "pr", "vx"):
+        assert rel_l2(a.grid[k], b.grid[k]) < 1e-8, k
+
+
+def test_mixed_precision_matches_fp64_and_oracle(pkg, oracle, built_lib, state41):
+    """Mixed precision: FP32 multifrontal factors (tensor-core products with
+    three TF32 terms) inside FP64 refinement reach the same 1e-13 residual;
+    the solution agrees with the FP64 factors to 1e-9 and with the oracle to
+    1e-8 per field."""
+    mx, st_mx = _hydro_pass(pkg, state41, 0, fp32=1)
+    fp, st_fp = _hydro_pass(pkg, state41, 0, fp32=0)
+    assert st_mx.converged and st_mx.rel_residual <= 1e-13, st_mx.rel_residual
+    assert st_mx.iterations >= st_fp.iterations
+    so = state41.copy()
+    o = oracle.Oracle(so)
+    o.markers_to_nodes(so.timesum)
+    o.gravity()
+    o.hydromech_pass(so.dt, 1)
+    for k in FIELDS:
+        assert rel_l2(mx.grid[k], fp.grid[k]) < 1e-9, k
+        assert rel_l2(mx.grid[k], so.grid[k]) < 1e-8, k
+
+
+def test_mixed_precision_steps_141(pkg, built_lib):
+    """Three timesteps of the 141 x 141 workload with FP32 and with FP64
+    factors: marker positions agree to 1e-10 relative, fields to 1e-8."""
+    out = {}
+    for fp32 in (0, 1):
+        st = pkg.make_state("planetesimal_141")
+        sim = pkg.Simulation(st)
+        sim.set_solver_options(factor_fp32=fp32)
+        for ts in (1, 2, 3):
+            sim.step(ts)
+        sim.download()
+        sim.close()
+        out[fp32] = st
+    a, b = out[1], out[0]
     assert a.marknum == b.marknum
     n = a.marknum
     for k in ("xm", "ym"):
