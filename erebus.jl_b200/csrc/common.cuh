@@ -170,8 +170,11 @@ EREBUS_HD double u01(uint64_t seed, uint64_t stream, uint64_t idx) {
     return (double)(z >> 11) * 0x1.0p-53;
 }
 
+// Grid size for n items (at least one block: every kernel checks its
+// index against n, and an empty marker set is a valid input).
 inline int nblocks(int64_t n, int threads = kThreads) {
-    return (int)((n + threads - 1) / threads);
+    int64_t b = (n + threads - 1) / threads;
+    return b > 0 ? (int)b : 1;
 }
 
 }  // namespace erebus
