@@ -200,7 +200,7 @@ int erebus_check_params(const ErebusParams *p) {
     int rm = p->reaction_rate_coeff_mode;
     if (rm != 1 && rm != 2 && rm != 3 && rm != 9) return EREBUS_EINVAL;
     if (p->dtstep < 1 || p->titermax < 1 || p->nplast < 1) return EREBUS_EINVAL;
-    if (p->dsubgridt != 0.0 || p->dsubgrids != 0.0) return EREBUS_EINVAL;
+    if (!(p->dsubgridt >= 0.0) || !(p->dsubgrids >= 0.0)) return EREBUS_EINVAL;
     return EREBUS_OK;
 }
 

@@ -222,7 +222,8 @@ __global__ void k_sort_segments(SortPtrs S, int gr) {
 // ---------------------------------------------------------------------------
 // merge scatter
 // ---------------------------------------------------------------------------
-enum MergeMode { MM_SCATTER = 0, MM_REACTION = 1, MM_MELT = 2 };
+enum MergeMode { MM_SCATTER = 0, MM_REACTION = 1, MM_MELT = 2, MM_SUBGRID_S = 3,
+                 MM_SUBGRID_T = 4 };
 
 template <int GRID, int MODE>
 struct MergeFields;
@@ -280,6 +281,34 @@ struct MergeFields<GP, MM_MELT> {
     __device__ static void load(const MP &M, const double *, const double *, int m,
                                 double v[N]) {
         v[0] = M.f[M_XWsolidm0][m]; v[1] = 1.0;
+    }
+};
+
+// subgrid stress diffusion (E:4309-4320): SXXSUM/WTPSUM on P nodes and
+// SXYSUM/WTSUM on basic nodes of the marker corrections (dM: xx, dH: xy)
+template <>
+struct MergeFields<GP, MM_SUBGRID_S> {
+    static constexpr int N = 2;
+    __device__ static void load(const MP &, const double *dM, const double *, int m,
+                                double v[N]) {
+        v[0] = dM[m]; v[1] = 1.0;
+    }
+};
+template <>
+struct MergeFields<GB, MM_SUBGRID_S> {
+    static constexpr int N = 2;
+    __device__ static void load(const MP &, const double *, const double *dH, int m,
+                                double v[N]) {
+        v[0] = dH[m]; v[1] = 1.0;
+    }
+};
+// subgrid temperature diffusion (E:4750-4751): TKSUM, RHOCPSUM
+template <>
+struct MergeFields<GP, MM_SUBGRID_T> {
+    static constexpr int N = 2;
+    __device__ static void load(const MP &, const double *dM, const double *dH, int m,
+                                double v[N]) {
+        v[0] = dM[m]; v[1] = dH[m];
     }
 };
 
@@ -377,6 +406,16 @@ __global__ void k_merge(Geo g, MP M, MergeArgs a, GPtr G, int write_props) {
             G.f[G_PHI][node] = phi;
             G.f[G_BETAPHI][node] = (1.0 / gggp) * phi;
         }
+    } else if (MODE == MM_SUBGRID_S && GRID == GP) {
+        // DSXX at inner P nodes (E:4323-4326)
+        if (I >= 2 && I <= g.Ny && J >= 2 && J <= g.Nx && wt > 0.0)
+            G.f[G_DSXX][node] -= acc[0] / wt;
+    } else if (MODE == MM_SUBGRID_S) {
+        // DSXY at all basic nodes (E:4328-4329)
+        if (wt > 0.0) G.f[G_DSXY][node] -= acc[0] / wt;
+    } else if (MODE == MM_SUBGRID_T) {
+        // DT -= TKSUM / RHOCPSUM (E:4754-4758)
+        if (wt > 0.0) G.f[G_DT][node] -= acc[0] / wt;
     } else if (MODE == MM_REACTION) {
         // compute_thermodynamic_xfer! (E:2208-2222)
         if (wt > 0.0) {
@@ -589,6 +628,61 @@ __device__ __forceinline__ double etatotal_rocks(const ErebusParams &p, double t
     return jmax(jmax(p.etamin, es), ef);
 }
 
+// apply_subgrid_stress_diffusion! (E:4253-4333), marker part: the
+// marker-node differences of sxx (P grid) and sxy (basic grid) relaxed over
+// dt with the reference's viscosity factor 1 (E:4276); markers corrected,
+// corrections to dM (xx) and dH (xy) for the marker-order node sums.
+__global__ void k_subgrid_stress(ErebusParams p, Geo g, MP M, GPtr G, int n, double dt,
+                                 double *dM, double *dH) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    const double etam = 1.0;
+    double x = M.f[M_xm][m], y = M.f[M_ym][m], w[4];
+    int i, j;
+    double relax = exp(-p.dsubgrids * dt / (etam * M.f[M_inv_gggtotalm][m])) - 1.0;
+    grid_weights(g, GP, x, y, i, j, w);
+    double d = M.f[M_sxxm][m] - gather4(G.f[G_SXX0], g.Ny1, i, j, w);
+    d *= relax;
+    M.f[M_sxxm][m] += d;
+    dM[m] = d;
+    grid_weights(g, GB, x, y, i, j, w);
+    d = M.f[M_sxym][m] - gather4(G.f[G_SXY0], g.Ny, i, j, w);
+    d *= relax;
+    M.f[M_sxym][m] += d;
+    dH[m] = d;
+}
+
+// apply_subgrid_temperature_diffusion! (E:4710-4761), marker part: the
+// marker-node temperature difference relaxed over dt with the marker's
+// conductivity and heat capacity (the algorithm the reference test verifies,
+// T:5480-5545; the reference body itself fails for rock markers), marker
+// corrected; dM = correction * rhocp, dH = rhocp for the node sums.
+__global__ void k_subgrid_temp(ErebusParams p, Geo g, MP M, GPtr G, int n, double dt,
+                               double *dM, double *dH) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    double x = M.f[M_xm][m], y = M.f[M_ym][m], w[4];
+    int i, j;
+    grid_weights(g, GP, x, y, i, j, w);
+    double tk = M.f[M_tkm][m];
+    double d = tk - gather4(G.f[G_tk1], g.Ny1, i, j, w);
+    int t = M.tm[m];
+    double rcp, k;
+    if (t < 3) {
+        double ph = M.f[M_phim][m];
+        rcp = total(p.rhocpsolidm[t - 1], rhocpfluid(p, tk), ph);
+        k = ktotal(ksolid(p, tk), kfluid(p, tk), ph);
+    } else {
+        rcp = p.rhocpsolidm[t - 1];
+        k = p.ksolidm[t - 1];
+    }
+    const double geom = 2.0 * (1.0 / (g.dx * g.dx) + 1.0 / (g.dy * g.dy));
+    d *= exp(-p.dsubgridt * k * dt / rcp * geom) - 1.0;
+    M.f[M_tkm][m] = tk + d;
+    dM[m] = d * rcp;
+    dH[m] = rcp;
+}
+
 // update_marker_viscosity! (E:774-804) and update_marker_stress! (E:4354-4388)
 __global__ void k_marker_visc_stress(ErebusParams p, Geo g, MP M, GPtr G, int n) {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -645,16 +739,30 @@ int nodes_to_markers(erebus_state *s, double dt, int timestep) {
     size_t np = (size_t)s->g.Nx1 * s->g.Ny1;
     cudaMemcpyAsync(s->grid[G_DT0], s->grid[G_DT], np * 8, cudaMemcpyDeviceToDevice,
                     s->stream);
-    if (n > 0) {
-        EREBUS_LAUNCH(s, k_marker_visc_stress, nblocks(n), kThreads, 0, s->p, s->g,
-                      mptr(s), gptr(s), n);
-        EREBUS_LAUNCH(s, k_marker_temp_poro, nblocks(n), kThreads, 0, s->p, s->g,
-                      mptr(s), gptr(s), n, dt, timestep);
-    }
     if (!s->sorted_valid) {
         int rc = build_cell_sort(s);
         if (rc) return rc;
     }
+    // The subgrid stress diffusion touches neither the viscosities nor what
+    // they read, so it runs before the combined viscosity + stress kernel,
+    // i.e. between update_marker_viscosity! and update_marker_stress! as in
+    // E:6950-6981; likewise the subgrid temperature diffusion before
+    // update_marker_temperature! (E:6986-7004).
+    if (s->p.dsubgrids != 0.0) {
+        EREBUS_LAUNCH(s, k_subgrid_stress, nblocks(n), kThreads, 0, s->p, s->g, mptr(s),
+                      gptr(s), n, dt, s->r_dM, s->r_dH);
+        launch_merge<GP, MM_SUBGRID_S>(s, merge_args(s, GP, {S_SXXSUM, S_WTPSUM}), 1);
+        launch_merge<GB, MM_SUBGRID_S>(s, merge_args(s, GB, {S_SXYSUM, S_WTSUM}), 1);
+    }
+    EREBUS_LAUNCH(s, k_marker_visc_stress, nblocks(n), kThreads, 0, s->p, s->g, mptr(s),
+                  gptr(s), n);
+    if (s->p.dsubgridt != 0.0) {
+        EREBUS_LAUNCH(s, k_subgrid_temp, nblocks(n), kThreads, 0, s->p, s->g, mptr(s),
+                      gptr(s), n, dt, s->r_dM, s->r_dH);
+        launch_merge<GP, MM_SUBGRID_T>(s, merge_args(s, GP, {S_TKSUM, S_RHOCPSUM}), 1);
+    }
+    EREBUS_LAUNCH(s, k_marker_temp_poro, nblocks(n), kThreads, 0, s->p, s->g, mptr(s),
+                  gptr(s), n, dt, timestep);
     // update_p_nodes_melt_composition! (E:1929-1939)
     launch_merge<GP, MM_MELT>(s, merge_args(s, GP, {S_XWSSUM, S_WTPSUM}), 1);
     return check_cuda(s, cudaGetLastError(), "nodes_to_markers");

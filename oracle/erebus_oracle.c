@@ -1083,6 +1083,89 @@ int64_t oracle_assemble_thermal(const ErebusParams *p, const ErebusGridHost *G,
    update_marker_porosity! (E:4822-4856), copy E:7014,
    update_p_nodes_melt_composition! (E:1929-1939).  The marker loops the
    reference runs with @threads run with OpenMP here. */
+/* apply_subgrid_stress_diffusion! (E:4253-4333): marker-node stress
+   differences relaxed over dt (the reference fixes the viscosity factor to
+   1, E:4276), markers corrected, the corrections scattered in marker order
+   and subtracted from DSXX at inner P nodes and from DSXY at all basic
+   nodes.  A no-op when dsubgrids == 0. */
+int oracle_subgrid_stress(const ErebusParams *p, ErebusMarkersHost *M, int64_t marknum,
+                          ErebusGridHost *G, ErebusSumsHost *s, double dt) {
+    if (p->dsubgrids == 0.0) return 0;
+    Geo g = geo(p);
+    int Ny = g.Ny, Ny1 = g.Ny1;
+    size_t np = (size_t)g.Nx1 * Ny1, nb = (size_t)g.Nx * Ny;
+    memset(s->SXXSUM, 0, np * 8);
+    memset(s->WTPSUM, 0, np * 8);
+    memset(s->SXYSUM, 0, nb * 8);
+    memset(s->WTSUM, 0, nb * 8);
+    const double etam = 1.0;
+    for (int64_t m = 0; m < marknum; m++) {
+        int ip, jp, ib, jb;
+        double wp[4], wb[4];
+        grid_weights(&g, GP, M->xm[m], M->ym[m], &ip, &jp, wp);
+        grid_weights(&g, GB, M->xm[m], M->ym[m], &ib, &jb, wb);
+        double dxx = M->sxxm[m] - gather4(G->SXX0, Ny1, ip, jp, wp);
+        dxx *= exp(-p->dsubgrids * dt / (etam * M->inv_gggtotalm[m])) - 1.0;
+        M->sxxm[m] += dxx;
+        add_to_grid(s->SXXSUM, Ny1, ip, jp, wp, dxx);
+        add_to_grid(s->WTPSUM, Ny1, ip, jp, wp, 1.0);
+        double dxy = M->sxym[m] - gather4(G->SXY0, Ny, ib, jb, wb);
+        dxy *= exp(-p->dsubgrids * dt / (etam * M->inv_gggtotalm[m])) - 1.0;
+        M->sxym[m] += dxy;
+        add_to_grid(s->SXYSUM, Ny, ib, jb, wb, dxy);
+        add_to_grid(s->WTSUM, Ny, ib, jb, wb, 1.0);
+    }
+    for (int j = 2; j <= g.Nx; j++)
+        for (int i = 2; i <= Ny; i++)
+            if (AT(s->WTPSUM, Ny1, i, j) > 0.0)
+                AT(G->DSXX, Ny1, i, j) -= AT(s->SXXSUM, Ny1, i, j) / AT(s->WTPSUM, Ny1, i, j);
+    for (size_t k = 0; k < nb; k++)
+        if (s->WTSUM[k] > 0.0) G->DSXY[k] -= s->SXYSUM[k] / s->WTSUM[k];
+    return 0;
+}
+
+/* apply_subgrid_temperature_diffusion! (E:4710-4761): marker-node
+   temperature differences relaxed over dt with the marker's conductivity
+   and heat capacity, markers corrected, the energy corrections scattered in
+   marker order, and DT -= TKSUM / RHOCPSUM.  For rock markers the reference
+   body assigns the conductivity to a loop-local name in one branch and
+   indexes it in the other, which Julia rejects (UndefVarError) whenever
+   dsubgridt > 0; this restatement follows the algorithm its test verifies
+   (HTM-planetary.m line 1731ff, T:5480-5545) with the conductivity and heat
+   capacity laws of compute_marker_properties!.  A no-op when dsubgridt == 0. */
+int oracle_subgrid_temperature(const ErebusParams *p, ErebusMarkersHost *M, int64_t marknum,
+                               ErebusGridHost *G, ErebusSumsHost *s, double dt) {
+    if (p->dsubgridt == 0.0) return 0;
+    Geo g = geo(p);
+    int Ny1 = g.Ny1;
+    size_t np = (size_t)g.Nx1 * Ny1;
+    memset(s->TKSUM, 0, np * 8);
+    memset(s->RHOCPSUM, 0, np * 8);
+    const double geom = 2.0 * (1.0 / (g.dx * g.dx) + 1.0 / (g.dy * g.dy));
+    for (int64_t m = 0; m < marknum; m++) {
+        int i, j;
+        double w[4];
+        grid_weights(&g, GP, M->xm[m], M->ym[m], &i, &j, w);
+        double d = M->tkm[m] - gather4(G->tk1, Ny1, i, j, w);
+        int t = (int)M->tm[m];
+        double tk = M->tkm[m], rcp, k;
+        if (t < 3) {
+            rcp = total(p->rhocpsolidm[t - 1], rhocpfluid(p, tk), M->phim[m]);
+            k = ktotal(ksolid(p, tk), kfluid(p, tk), M->phim[m]);
+        } else {
+            rcp = p->rhocpsolidm[t - 1];
+            k = p->ksolidm[t - 1];
+        }
+        d *= exp(-p->dsubgridt * k * dt / rcp * geom) - 1.0;
+        M->tkm[m] += d;
+        add_to_grid(s->TKSUM, Ny1, i, j, w, d * rcp);
+        add_to_grid(s->RHOCPSUM, Ny1, i, j, w, rcp);
+    }
+    for (size_t q = 0; q < np; q++)
+        if (s->RHOCPSUM[q] > 0.0) G->DT[q] -= s->TKSUM[q] / s->RHOCPSUM[q];
+    return 0;
+}
+
 int oracle_nodes_to_markers(const ErebusParams *p, ErebusMarkersHost *M,
                             int64_t marknum, ErebusGridHost *G,
                             ErebusSumsHost *s, double dt, int timestep) {
@@ -1107,6 +1190,7 @@ int oracle_nodes_to_markers(const ErebusParams *p, ErebusMarkersHost *M,
             M->etavpm[m] = M->etatotalm[m];
         }
     }
+    oracle_subgrid_stress(p, M, marknum, G, s, dt);
 #pragma omp parallel for schedule(static)
     for (int64_t m = 0; m < marknum; m++) {
         int ip, jp, ib, jb;
@@ -1118,6 +1202,7 @@ int oracle_nodes_to_markers(const ErebusParams *p, ErebusMarkersHost *M,
         M->sxxm[m] += gather4(G->DSXX, Ny1, ip, jp, wp);
         M->sxym[m] += gather4(G->DSXY, Ny, ib, jb, wb);
     }
+    oracle_subgrid_temperature(p, M, marknum, G, s, dt);
 #pragma omp parallel for schedule(static)
     for (int64_t m = 0; m < marknum; m++) {
         int i, j;

@@ -104,6 +104,8 @@ def lib():
             "oracle_scatter_only": (None, [P, P, I64, P]),
             "oracle_node_properties": (None, [P, P, P]),
             "oracle_insulating_bc": (None, [P, P]),
+            "oracle_subgrid_stress": (I, [P, P, I64, P, P, D]),
+            "oracle_subgrid_temperature": (I, [P, P, I64, P, P, D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -69,7 +69,9 @@ def test_check_params_rejects_bad_sets(pkg, built_lib):
     p.marker_property_mode = 3
     assert built_lib.erebus_check_params(ctypes.byref(p)) == 1
     p = pkg.default_params(15, 15)
-    p.dsubgrids = 1.0    # subgrid diffusion is not part of the device path
+    p.dsubgrids = 1.0    # subgrid diffusion is part of the device path
+    assert built_lib.erebus_check_params(ctypes.byref(p)) == 0
+    p.dsubgridt = -1.0   # but a negative diffusion coefficient is not a valid set
     assert built_lib.erebus_check_params(ctypes.byref(p)) == 1
 
 

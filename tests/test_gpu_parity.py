@@ -172,3 +172,29 @@ def test_replenish_matches_oracle(pkg, oracle, built_lib, advanced):
     for k in ["xm", "ym", "tm", "tkm", "phim", "sxxm", "etavpm"]:
         np.testing.assert_array_equal(sg.m[k][:ng], so.m[k][:ng], err_msg=k)
     sim.close()
+
+
+def test_subgrid_diffusion_step(pkg, oracle, built_lib):
+    """A timestep with subgrid stress and temperature diffusion switched on
+    (dsubgrids, dsubgridt > 0; the reference's defaults are 0): the marker
+    stresses, temperatures and positions and the stress and temperature
+    changes on the nodes agree with the oracle as in the other step tests."""
+    st = pkg.make_state(CFG)
+    st.p.dsubgrids = 1e-21      # relaxation factors of order one at dt ~ 1e11 s
+    st.p.dsubgridt = 1e-3
+    o = oracle.Oracle(st)
+    o.step(1)
+    so, o, sg, sim = _pair(pkg, oracle, st)
+    so_stats = o.step(2)
+    gs = sim.step(2)
+    sim.download()
+    sim.close()
+    assert gs.titer == so_stats["titer"]
+    n = so.marknum
+    assert sg.marknum == n
+    for k in ["xm", "ym"]:
+        assert rel_linf(sg.m[k][:n], so.m[k][:n]) <= 1e-10, k
+    for k in ["sxxm", "sxym", "tkm"]:
+        assert rel_linf(sg.m[k][:n], so.m[k][:n]) <= 1e-8, k
+    for k in ["DSXX", "DSXY", "DT", "tk2"]:
+        assert rel_l2(sg.grid[k], so.grid[k]) <= 1e-8, k

@@ -1097,3 +1097,114 @@ def test_replenish(L, P, G, pkg):
               "XWsolidm", "XWsolidm0"):
         np.testing.assert_array_equal(m[k][:n], before[k], err_msg=k)
         np.testing.assert_array_equal(m[k][n:n_new], before[k][src], err_msg=k)
+
+
+# ---------------------------------------------------------------------------
+# subgrid diffusion (T:5033-5200, T:5460-5553)
+# ---------------------------------------------------------------------------
+def _subgrid_state(pkg, P, G, rng):
+    n = G.start_marknum
+    st = pkg.HostState(P, capacity=n)
+    m = st.m
+    m["xm"][:] = -G.dx + rng.integers(0, int((G.xsize + 2 * G.dx) / 0.1) + 1, n) * 0.1
+    m["ym"][:] = -G.dy + rng.integers(0, int((G.ysize + 2 * G.dy) / 0.1) + 1, n) * 0.1
+    m["tm"][:] = rng.integers(1, 4, n)
+    for k in ("sxxm", "sxym", "tkm", "phim"):
+        m[k][:] = rng.random(n)
+    m["inv_gggtotalm"][:] = 1.0 / (1e10 * (0.5 + rng.random(n)))
+    st.marknum = n
+    for k in ("SXX0", "SXY0", "DSXX", "DSXY", "tk1", "DT"):
+        st.grid[k][:] = rng.random(st.grid[k].shape)
+    return st
+
+
+def test_subgrid_stress_diffusion(L, G, pkg):
+    """apply_subgrid_stress_diffusion! against HTM-planetary.m line 1374ff as
+    T:5076-5198 states it, with dsubgrids = 1 (the reference's default 0
+    makes it a no-op) and the reference's viscosity factor 1 (E:4276):
+    relaxation time 1 / G per marker."""
+    rng = np.random.default_rng(5033)
+    p = pkg.params.default_params(15, 15)
+    p.dsubgrids = 1.0
+    st = _subgrid_state(pkg, p, G, rng)
+    m, g = st.m, st.grid
+    n = st.marknum
+    dt = 1e-3
+    sxx, sxy = m["sxxm"][:n].copy(), m["sxym"][:n].copy()
+    DSXX, DSXY = g["DSXX"].copy(), g["DSXY"].copy()
+    L.oracle_subgrid_stress(_ref(p), _ref(st.markers_struct()), n, _ref(st.grid_struct()),
+                            _ref(st.sums_struct()), dt)
+    SXXSUM = np.zeros((G.Ny1, G.Nx1)); WTPSUM = np.zeros((G.Ny1, G.Nx1))
+    SXYSUM = np.zeros((G.Ny, G.Nx)); WTSUM = np.zeros((G.Ny, G.Nx))
+    for q in range(n):
+        ggg = 1.0 / m["inv_gggtotalm"][q]
+        relax = math.exp(-p.dsubgrids * dt / (1.0 / ggg))
+        for grid, val, S, W in ((3, sxx, SXXSUM, WTPSUM), (0, sxy, SXYSUM, WTSUM)):
+            xa, ya, jmax, imax = _grids(G)[grid]
+            i, j = _fix_ver(m["xm"][q], m["ym"][q], xa, ya, G.dx, G.dy, jmax, imax)
+            dxmj, dymi = m["xm"][q] - xa[j - 1], m["ym"][q] - ya[i - 1]
+            w = [(1 - dxmj / G.dx) * (1 - dymi / G.dy), (1 - dxmj / G.dx) * (dymi / G.dy),
+                 (dxmj / G.dx) * (1 - dymi / G.dy), (dxmj / G.dx) * (dymi / G.dy)]
+            src = g["SXX0"] if grid == 3 else g["SXY0"]
+            cells = [(i - 1, j - 1), (i, j - 1), (i - 1, j), (i, j)]
+            d0 = val[q] - sum(src[c] * wc for c, wc in zip(cells, w))
+            dd = d0 * relax - d0
+            val[q] += dd
+            for c, wc in zip(cells, w):
+                S[c] += dd * wc
+                W[c] += wc
+    inner = np.zeros_like(WTPSUM, bool)
+    inner[1:G.Ny, 1:G.Nx] = True
+    nz = inner & (WTPSUM > 0)
+    DSXX[nz] -= SXXSUM[nz] / WTPSUM[nz]
+    nzb = WTSUM > 0
+    DSXY[nzb] -= SXYSUM[nzb] / WTSUM[nzb]
+    np.testing.assert_allclose(m["sxxm"][:n], sxx, rtol=RTOL)
+    np.testing.assert_allclose(m["sxym"][:n], sxy, rtol=RTOL)
+    np.testing.assert_allclose(g["DSXX"], DSXX, rtol=RTOL, atol=1e-12)
+    np.testing.assert_allclose(g["DSXY"], DSXY, rtol=RTOL, atol=1e-12)
+
+
+def test_subgrid_temperature_diffusion(L, G, pkg):
+    """apply_subgrid_temperature_diffusion! against HTM-planetary.m line
+    1731ff as T:5480-5550 states it, with dsubgridt = 1 and constant
+    material laws (mode 9)."""
+    rng = np.random.default_rng(5460)
+    p = pkg.params.default_params(15, 15)
+    p.dsubgridt = 1.0
+    st = _subgrid_state(pkg, p, G, rng)
+    m, g = st.m, st.grid
+    n = st.marknum
+    dt = 1e7
+    tk = m["tkm"][:n].copy()
+    DT = g["DT"].copy()
+    L.oracle_subgrid_temperature(_ref(p), _ref(st.markers_struct()), n,
+                                 _ref(st.grid_struct()), _ref(st.sums_struct()), dt)
+    TKSUM = np.zeros((G.Ny1, G.Nx1)); RCP = np.zeros((G.Ny1, G.Nx1))
+    rs, rf = list(p.rhocpsolidm), list(p.rhocpfluidm)
+    ks, kf = list(p.ksolidm), list(p.kfluidm)
+    for q in range(n):
+        i, j = _fix_ver(m["xm"][q], m["ym"][q], G.xp, G.yp, G.dx, G.dy, G.Nx, G.Ny)
+        dxmj, dymi = m["xm"][q] - G.xp[j - 1], m["ym"][q] - G.yp[i - 1]
+        w = [(1 - dxmj / G.dx) * (1 - dymi / G.dy), (1 - dxmj / G.dx) * (dymi / G.dy),
+             (dxmj / G.dx) * (1 - dymi / G.dy), (dxmj / G.dx) * (dymi / G.dy)]
+        cells = [(i - 1, j - 1), (i, j - 1), (i - 1, j), (i, j)]
+        d0 = tk[q] - sum(g["tk1"][c] * wc for c, wc in zip(cells, w))
+        t = int(m["tm"][q]) - 1
+        ph = m["phim"][q]
+        if t < 2:
+            rcp = rs[t] * (1 - ph) + rf[t] * ph
+            a = ks[t] * (3 * ph - 2) + kf[t] * (1 - 3 * ph)
+            k = (ks[t] * kf[t] / 2 + a ** 2 / 16) ** 0.5 - a / 4
+        else:
+            rcp, k = rs[t], ks[t]
+        d1 = d0 * math.exp(-p.dsubgridt * k * dt / rcp * (2 / G.dx ** 2 + 2 / G.dy ** 2))
+        dd = d1 - d0
+        tk[q] += dd
+        for c, wc in zip(cells, w):
+            TKSUM[c] += dd * rcp * wc
+            RCP[c] += rcp * wc
+    nz = RCP > 0
+    DT[nz] -= TKSUM[nz] / RCP[nz]
+    np.testing.assert_allclose(m["tkm"][:n], tk, rtol=RTOL)
+    np.testing.assert_allclose(g["DT"], DT, rtol=RTOL, atol=1e-12)
