@@ -198,3 +198,31 @@ def test_subgrid_diffusion_step(pkg, oracle, built_lib):
         assert rel_linf(sg.m[k][:n], so.m[k][:n]) <= 1e-8, k
     for k in ["DSXX", "DSXY", "DT", "tk2"]:
         assert rel_l2(sg.grid[k], so.grid[k]) <= 1e-8, k
+
+
+@pytest.mark.parametrize("mode,rmode", [(1, 1), (1, 2), (9, 3)])
+def test_material_and_reaction_modes(pkg, oracle, built_lib, mode, rmode):
+    """Temperature-dependent material laws (marker_property_mode 1:
+    Hobbs/Touloukian heat capacity and conductivities, E:2272-2358) and the
+    reaction-time modes 2 and 3 (E:2386-2389): two timesteps from the
+    initial state against the oracle."""
+    st = pkg.make_state(CFG)
+    st.p.marker_property_mode = mode
+    st.p.reaction_rate_coeff_mode = rmode
+    so, o, sg, sim = _pair(pkg, oracle, st)
+    for ts in (1, 2):
+        a = o.step(ts)
+        b = sim.step(ts)
+        assert a["titer"] == b.titer, ts
+    sim.download()
+    sim.close()
+    n = so.marknum
+    assert sg.marknum == n
+    for k in ["xm", "ym"]:
+        assert rel_linf(sg.m[k][:n], so.m[k][:n]) <= 1e-10, k
+    for k in ["tkm", "phim", "XWsolidm0"]:
+        assert rel_linf(sg.m[k][:n], so.m[k][:n]) <= 1e-8, k
+    # (DMP is left out: near equilibrium (1 - RV) / dt is rounding noise of
+    # order 1e-27 on both sides, E:2667)
+    for k in ["vx", "pr", "pf", "tk2"]:
+        assert rel_l2(sg.grid[k], so.grid[k]) <= 1e-8, k
