@@ -217,6 +217,14 @@ int erebus_destroy(erebus_state *s) {
     band_free(s->thermal);
     band_free(s->gravity);
     if (s->hsc) cudaFreeHost(s->hsc);
+    if (s->copy_stream) {
+        cudaStreamSynchronize(s->copy_stream);
+        cudaStreamDestroy(s->copy_stream);
+        cudaEventDestroy(s->snap_ready);
+        cudaEventDestroy(s->snap_done);
+    }
+    if (s->snap_dev) cudaFree(s->snap_dev);
+    if (s->snap_tm) cudaFreeHost(s->snap_tm);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return EREBUS_OK;
@@ -434,6 +442,101 @@ int erebus_download_sums(erebus_state *s, ErebusSumsHost *sh) {
                                           s->stream), "download sums"));
     }
     return check_cuda(s, cudaStreamSynchronize(s->stream), "download sums");
+}
+
+// save_state (E:5718-5960) every savematstep timesteps (E:7106): the state is
+// staged in device memory on the library's stream (so the following steps may
+// overwrite it at once) and drained to the caller's host buffers on a second
+// stream while the simulation goes on.
+int erebus_snapshot_begin(erebus_state *s, const ErebusGridHost *gh,
+                          const ErebusMarkersHost *mh) {
+    if (!s || !gh || !mh || s->snap_pending) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    const void *const *gd = reinterpret_cast<const void *const *>(gh);
+    for (int f = 0; f < G_COUNT; f++)
+        if (!gd[f]) return EREBUS_EINVAL;
+    const int64_t n = s->marknum;
+    size_t need = 0;
+    for (int f = 0; f < G_COUNT; f++) need += (field_bytes(s, f) + 255) / 256 * 256;
+    const size_t mbytes = ((size_t)s->capacity * 8 + 255) / 256 * 256;
+    need += (size_t)M_COUNT * mbytes;
+    if (!s->copy_stream) {
+        if (cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->snap_ready, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->snap_done, cudaEventDisableTiming) != cudaSuccess) {
+            s->last_error = "snapshot: stream or event creation failed";
+            return EREBUS_ECUDA;
+        }
+    }
+    if (s->snap_cap < need) {
+        if (s->snap_dev) cudaFree(s->snap_dev);
+        if (s->snap_tm) cudaFreeHost(s->snap_tm);
+        s->snap_dev = nullptr;
+        s->snap_tm = nullptr;
+        s->snap_cap = 0;
+        if (cudaMalloc(&s->snap_dev, need) != cudaSuccess ||
+            cudaMallocHost(&s->snap_tm, (size_t)s->capacity) != cudaSuccess) {
+            s->last_error = "snapshot: staging allocation failed";
+            return EREBUS_ENOMEM;
+        }
+        s->snap_cap = need;
+    }
+    // stage on the library's stream
+    char *p = s->snap_dev;
+    std::vector<char *> gst(G_COUNT), mst(M_COUNT);
+    for (int f = 0; f < G_COUNT; f++) {
+        gst[f] = p;
+        TRY(check_cuda(s, cudaMemcpyAsync(p, s->grid[f], field_bytes(s, f),
+                                          cudaMemcpyDeviceToDevice, s->stream), "snapshot"));
+        p += (field_bytes(s, f) + 255) / 256 * 256;
+    }
+    void *const *mdst = reinterpret_cast<void *const *>(mh);
+    for (int f = 0; f < M_COUNT; f++) {
+        mst[f] = p;
+        const void *src = f == M_tm ? (const void *)s->tm8 : (const void *)s->m[f];
+        size_t b = f == M_tm ? (size_t)n : (size_t)n * 8;
+        if (b && mdst[f]) TRY(check_cuda(s, cudaMemcpyAsync(p, src, b, cudaMemcpyDeviceToDevice,
+                                                 s->stream), "snapshot"));
+        p += mbytes;
+    }
+    TRY(check_cuda(s, cudaEventRecord(s->snap_ready, s->stream), "snapshot"));
+    // drain on the copy stream
+    TRY(check_cuda(s, cudaStreamWaitEvent(s->copy_stream, s->snap_ready, 0), "snapshot"));
+    void *const *gdst = reinterpret_cast<void *const *>(gh);
+    for (int f = 0; f < G_COUNT; f++)
+        TRY(check_cuda(s, cudaMemcpyAsync(gdst[f], gst[f], field_bytes(s, f),
+                                          cudaMemcpyDeviceToHost, s->copy_stream), "snapshot"));
+    for (int f = 0; f < M_COUNT; f++) {
+        if (f == M_tm) {
+            if (n && mh->tm) TRY(check_cuda(s, cudaMemcpyAsync(s->snap_tm, mst[f], (size_t)n,
+                                                     cudaMemcpyDeviceToHost, s->copy_stream),
+                                  "snapshot"));
+            continue;
+        }
+        if (!mdst[f] || !n) continue;
+        TRY(check_cuda(s, cudaMemcpyAsync(mdst[f], mst[f], (size_t)n * 8,
+                                          cudaMemcpyDeviceToHost, s->copy_stream), "snapshot"));
+    }
+    TRY(check_cuda(s, cudaEventRecord(s->snap_done, s->copy_stream), "snapshot"));
+    s->snap_tm_dst = mh->tm;
+    s->snap_marknum = n;
+    s->snap_dt = s->dt;
+    s->snap_timesum = s->timesum;
+    s->snap_pending = true;
+    return EREBUS_OK;
+}
+
+int erebus_snapshot_wait(erebus_state *s, int64_t *marknum, double *dt, double *timesum) {
+    if (!s || !s->snap_pending) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    s->snap_pending = false;
+    TRY(check_cuda(s, cudaEventSynchronize(s->snap_done), "snapshot wait"));
+    if (s->snap_tm_dst)
+        for (int64_t k = 0; k < s->snap_marknum; k++) s->snap_tm_dst[k] = s->snap_tm[k];
+    if (marknum) *marknum = s->snap_marknum;
+    if (dt) *dt = s->snap_dt;
+    if (timesum) *timesum = s->snap_timesum;
+    return EREBUS_OK;
 }
 
 int erebus_set_time(erebus_state *s, double dt, double timesum) {

@@ -120,6 +120,16 @@ struct erebus_state {
     int8_t *r_flag = nullptr;
     double *tmp_node = nullptr;                // node-sized scratch
     double *norm_part = nullptr;               // partial sums of the residual norms
+    // asynchronous snapshot (erebus_snapshot_begin / _wait)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
+    char *snap_dev = nullptr;                  // device staging copy of the state
+    int8_t *snap_tm = nullptr;                 // pinned host copy of the types
+    size_t snap_cap = 0;
+    bool snap_pending = false;
+    int64_t snap_marknum = 0;
+    double snap_dt = 0.0, snap_timesum = 0.0;
+    int64_t *snap_tm_dst = nullptr;
     double *partials = nullptr;                // reduction partials
     // replenishment scratch (per marker-grid anchor)
     unsigned long long *a_mdis = nullptr;

@@ -27,6 +27,7 @@ EXPORTS = [
     "erebus_hydromech_pass", "erebus_thermal_solve", "erebus_nodes_to_markers",
     "erebus_advect_rk4", "erebus_replenish", "erebus_step", "erebus_export_hydromech",
     "erebus_apply_hydromech", "erebus_kernel_launches", "erebus_factor_stats",
+    "erebus_snapshot_begin", "erebus_snapshot_wait",
 ]
 
 
@@ -66,6 +67,9 @@ def load_library(path=LIB_PATH):
         "erebus_upload_grid": [P, ctypes.POINTER(ErebusGridHost)],
         "erebus_download_grid": [P, ctypes.POINTER(ErebusGridHost)],
         "erebus_download_sums": [P, ctypes.POINTER(ErebusSumsHost)],
+        "erebus_snapshot_begin": [P, ctypes.POINTER(ErebusGridHost),
+                                  ctypes.POINTER(ErebusMarkersHost)],
+        "erebus_snapshot_wait": [P, pI64, pD, pD],
         "erebus_set_time": [P, D, D],
         "erebus_get_time": [P, pD, pD],
         "erebus_markers_to_nodes": [P, D],
@@ -159,6 +163,27 @@ class Simulation:
         self._check("erebus_download_sums", self.L.erebus_download_sums(
             self.h, ctypes.byref(st.sums_struct())))
         return st.sums
+
+    def snapshot_begin(self, buffers):
+        """Starts an asynchronous copy of the state (markers, grid, marknum,
+        dt, timesum) into `buffers`, a HostState of the same geometry, and
+        returns at once; steps may follow while the copy runs.  Buffers made
+        with HostState(..., pinned=True) let the copy overlap the steps.
+        The snapshot is the input of save_state (E:5718-5960)."""
+        self._check("erebus_snapshot_begin", self.L.erebus_snapshot_begin(
+            self.h, ctypes.byref(buffers.grid_struct()),
+            ctypes.byref(buffers.markers_struct())))
+        self._snapshot = buffers
+
+    def snapshot_wait(self):
+        """Waits for the copy started by `snapshot_begin`; returns its buffers
+        with marknum, dt and timesum as they were when it began."""
+        n, dt, ts = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        self._check("erebus_snapshot_wait", self.L.erebus_snapshot_wait(
+            self.h, ctypes.byref(n), ctypes.byref(dt), ctypes.byref(ts)))
+        b, self._snapshot = self._snapshot, None
+        b.marknum, b.dt, b.timesum = n.value, dt.value, ts.value
+        return b
 
     def set_solver_options(self, **kw):
         o = ErebusSolverOptions()
@@ -280,20 +305,49 @@ class Simulation:
         return v.value or 0
 
 
-def run_simulation(host, n_steps, start_step=1, callback=None):
-    """The reference's simulation_loop over `n_steps` timesteps on the GPU
-    (without snapshot output).  Returns the list of ErebusStepStats."""
+def run_simulation(host, n_steps, start_step=1, callback=None, output_path=None,
+                   savematstep=10):
+    """The reference's simulation_loop over `n_steps` timesteps on the GPU.
+    Returns the list of ErebusStepStats.
+
+    With `output_path`, the state after every timestep divisible by
+    `savematstep` is written as output_<timestep>.npz (save_state,
+    E:7106-7235): the snapshot is copied out on a second stream while the
+    next timestep runs, and a writer thread saves it."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from .host import HostState
+    from .output import save_state
+
     sim = Simulation(host)
     out = []
+    pool = ThreadPoolExecutor(max_workers=1) if output_path is not None else None
+    buffers, pending, written = None, None, None
     try:
         for ts in range(start_step, start_step + n_steps):
             s = sim.step(ts)
             out.append(s)
+            if pending is not None:
+                written = pool.submit(save_state, output_path, pending, sim.snapshot_wait())
+                pending = None
             if callback:
                 callback(ts, s)
+            if output_path is not None and ts % savematstep == 0:
+                if written is not None:
+                    written.result()
+                if buffers is None:
+                    buffers = HostState(host.p, host.capacity, pinned=True)
+                sim.snapshot_begin(buffers)
+                pending = ts
             if s.timesum > host.p.endtime:
                 break
+        if pending is not None:
+            written = pool.submit(save_state, output_path, pending, sim.snapshot_wait())
+        if written is not None:
+            written.result()
         sim.download()
     finally:
+        if pool is not None:
+            pool.shutdown()
         sim.close()
     return out

@@ -56,30 +56,44 @@ def u01(seed, stream, idx):
 
 
 class HostState:
-    """Numpy arrays for one planetesimal, plus ctypes views of them."""
+    """Numpy arrays for one planetesimal, plus ctypes views of them.
 
-    def __init__(self, p, capacity=None):
+    With `pinned`, the marker and grid arrays live in page-locked host memory
+    (allocated through torch), which lets device copies run asynchronously."""
+
+    def __init__(self, p, capacity=None, pinned=False):
         self.p = p
         self.g = g = Geometry(p)
         if capacity is None:
             capacity = int(g.start_marknum * 1.25) + 1024
         self.capacity = int(capacity)
         self.marknum = 0
+        self._pins = []
+        zeros = self._pinned_zeros if pinned else (
+            lambda shape, dtype, order="C": np.zeros(shape, dtype=dtype, order=order))
         self.m = {}
         for name in MARKER_FIELDS:
             dt = np.int64 if name == "tm" else np.float64
-            self.m[name] = np.zeros(self.capacity, dtype=dt)
+            self.m[name] = zeros(self.capacity, dt)
         self.grid = {}
         for name in GRID_FIELDS:
             shape = (g.Ny, g.Nx) if name in BASIC_GRID else (g.Ny1, g.Nx1)
             dt = np.uint8 if name in BOOL_GRID else np.float64
-            self.grid[name] = np.zeros(shape, dtype=dt, order="F")
+            self.grid[name] = zeros(shape, dt, order="F")
         self.sums = {}
         for name in SUM_FIELDS:
             shape = (g.Ny, g.Nx) if name in BASIC_SUMS else (g.Ny1, g.Nx1)
             self.sums[name] = np.zeros(shape, dtype=np.float64, order="F")
         self.dt = p.dt_longest          # setup_dynamic_simulation_parameters
         self.timesum = p.start_time     # (E:55-70)
+
+    def _pinned_zeros(self, shape, dtype, order="C"):
+        import torch
+        dtype = np.dtype(dtype)
+        n = int(np.prod(shape))
+        t = torch.zeros(max(n, 1) * dtype.itemsize, dtype=torch.uint8, pin_memory=True)
+        self._pins.append(t)
+        return t.numpy()[: n * dtype.itemsize].view(dtype).reshape(shape, order=order)
 
     # -- ctypes views -----------------------------------------------------
     @staticmethod
@@ -110,6 +124,7 @@ class HostState:
     def copy(self):
         o = HostState.__new__(HostState)
         o.p, o.g, o.capacity, o.marknum = self.p, self.g, self.capacity, self.marknum
+        o._pins = []
         o.m = {k: v.copy() for k, v in self.m.items()}
         o.grid = {k: v.copy(order="F") for k, v in self.grid.items()}
         o.sums = {k: v.copy(order="F") for k, v in self.sums.items()}

@@ -239,6 +239,21 @@ int erebus_download_markers(erebus_state *s, ErebusMarkersHost *m,
 int erebus_upload_grid(erebus_state *s, const ErebusGridHost *g);
 int erebus_download_grid(erebus_state *s, ErebusGridHost *g);
 int erebus_download_sums(erebus_state *s, ErebusSumsHost *sums);
+/* Asynchronous snapshot of the state for save_state (src/Erebus.jl:5718-5960,
+   written every savematstep timesteps, src/Erebus.jl:7106).  _begin stages
+   every grid field and the marker arrays whose pointer is non-NULL in device
+   memory, in stream order after the work already issued, and drains them to
+   the given host buffers on a second stream; it returns at once, and steps
+   may follow while the copies run.  Every grid pointer must be non-NULL.
+   Host buffers must stay valid until _wait, and must be page-locked for the
+   copies to overlap the steps (pageable buffers make _begin wait for them).
+   _wait blocks until the copies have landed, widens tm to int64 and returns
+   marknum, dt and timesum as they were at _begin.  EREBUS_EINVAL: _begin
+   while a snapshot is pending, or _wait with none pending. */
+int erebus_snapshot_begin(erebus_state *s, const ErebusGridHost *g,
+                          const ErebusMarkersHost *m);
+int erebus_snapshot_wait(erebus_state *s, int64_t *marknum, double *dt,
+                         double *timesum);
 /* dt / timesum / timestep counters of the device-side driver. */
 int erebus_set_time(erebus_state *s, double dt, double timesum);
 int erebus_get_time(const erebus_state *s, double *dt, double *timesum);
