@@ -161,6 +161,14 @@ class ErebusFactorStats(Structure):
     ]
 
 
+class ErebusAdjointStats(Structure):
+    _fields_ = [
+        ("steps", c_int32), ("checkpoints", c_int32), ("adjoint_solves", c_int32),
+        ("factorizations", c_int32), ("markers", c_int64), ("J", c_double),
+        ("body_nodes", c_double),
+    ]
+
+
 class ErebusSolverOptions(Structure):
     _fields_ = [
         ("hydro_rtol", c_double), ("thermal_rtol", c_double),

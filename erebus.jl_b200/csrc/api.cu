@@ -216,6 +216,8 @@ int erebus_destroy(erebus_state *s) {
     band_free(s->hydro);
     band_free(s->thermal);
     band_free(s->gravity);
+    band_free(s->heat_adjoint);
+    if (s->adj_mem) cudaFree(s->adj_mem);
     if (s->hsc) cudaFreeHost(s->hsc);
     if (s->copy_stream) {
         cudaStreamSynchronize(s->copy_stream);

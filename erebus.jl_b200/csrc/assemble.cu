@@ -337,21 +337,28 @@ int assemble_system(erebus_state *s, int kind) {
     rc = check_cuda(s, cudaStreamSynchronize(s->stream), "assemble");
     if (rc) return rc;
     if (changed || !sys.factored || !s->opt.reuse_factors) {
-        if (use_multifrontal(s)) {
-            // the multifrontal factorisation reads the ELL entries itself
-            rc = check_cuda(s, cudaMemcpyAsync(sys.ell_prev, sys.ell_vals,
+        rc = commit_assembly(s, sys);
+        if (rc) return rc;
+    }
+    return check_cuda(s, cudaGetLastError(), "assemble");
+}
+
+int commit_assembly(erebus_state *s, BandSystem &sys) {
+    int64_t rows = (int64_t)sys.NB * sys.nb;
+    if (use_multifrontal(s)) {
+        // the multifrontal factorisation reads the ELL entries itself
+        int rc = check_cuda(s, cudaMemcpyAsync(sys.ell_prev, sys.ell_vals,
                                                rows * sys.ell * sizeof(double),
                                                cudaMemcpyDeviceToDevice, s->stream),
                             "assemble");
-            if (rc) return rc;
-        } else {
-            rc = band_zero(s, sys);   // allocates the band storage on first use
-            if (rc) return rc;
-            EREBUS_LAUNCH(s, k_ell_to_band, nblocks(rows, 128), 128, 0, band_view(sys),
-                          sys.ell_prev);
-        }
-        sys.factored = false;
+        if (rc) return rc;
+    } else {
+        int rc = band_zero(s, sys);   // allocates the band storage on first use
+        if (rc) return rc;
+        EREBUS_LAUNCH(s, k_ell_to_band, nblocks(rows, 128), 128, 0, band_view(sys),
+                      sys.ell_prev);
     }
+    sys.factored = false;
     return check_cuda(s, cudaGetLastError(), "assemble");
 }
 

@@ -15,6 +15,7 @@
 //   backtrace_pressures_rk4! (E:5284);
 // * replenish_markers! (E:5586) as per-anchor reductions plus a prefix sum.
 #include <climits>
+#include "laws.cuh"
 #include "state.cuh"
 
 namespace erebus {
@@ -37,72 +38,6 @@ static GPtr gptr(erebus_state *s) {
     GPtr r;
     for (int k = 0; k < G_COUNT; k++) r.f[k] = s->grid[k];
     return r;
-}
-
-// ---------------------------------------------------------------------------
-// material laws (E:1116-1275, E:2272-2397)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double total(double s, double f, double phi) {
-    return s * (1.0 - phi) + f * phi;
-}
-__device__ __forceinline__ double ktotal(double ks, double kf, double phi) {
-    double a = ks * (3.0 * phi - 2.0) + kf * (1.0 - 3.0 * phi);
-    return sqrt(ks * kf / 2 + (a * a) * (1.0 / 16.0)) -
-           0.25 * (ks * (3.0 * phi - 2.0) + kf * (1.0 - 3.0 * phi));
-}
-// x^3 with one final rounding of a compensated product (Julia evaluates a
-// Float64 power with an integral exponent by compensated repeated
-// multiplication); x^2 is a single correctly rounded product.
-__device__ __forceinline__ double cube(double x) {
-    double hi = x * x, lo = fma(x, x, -hi);
-    double p = hi * x, e = fma(hi, x, -p);
-    return p + (e + lo * x);
-}
-__device__ __forceinline__ double etaf_inv_kphi(const ErebusParams &p, double k0,
-                                                double phi, double etaf) {
-    double r = (1.0 - phi) * (1.0 / (1.0 - p.phim0));
-    return etaf * (1.0 / k0) * cube(p.phim0 * (1.0 / phi)) * (r * r);
-}
-__device__ __forceinline__ double rhocpfluid(const ErebusParams &p, double T) {
-    if (p.marker_property_mode == 1) {
-        double tm = p.tmfluidphase;
-        if (T < tm - 5.0) return p.rhoH2Ofi * (7.67 * T);
-        if (T < tm) return p.rhoH2Ofi * (7.67 * T + 0.1 * p.Lf);
-        if (T < tm + 5.0) return p.rhoH2Of * (4200.0 + 0.1 * p.Lf);
-        if (T < 410.0) return p.rhoH2Of * 4200.0;
-        return p.rhoH2Of *
-               (-4.67e4 + 333 * T - 0.731 * (T * T) + 5.4e-4 * (T * T * T));
-    }
-    return p.rhocpfluidm[0];
-}
-__device__ __forceinline__ double ksolid(const ErebusParams &p, double T) {
-    if (p.marker_property_mode == 1) return 0.73 + 1293.0 / (T + 77.0);
-    return p.ksolidm[0];
-}
-__device__ __forceinline__ double kfluid(const ErebusParams &p, double T) {
-    if (p.marker_property_mode == 1) {
-        if (T < p.tmfluidphase) return 0.465 + 488.0 / T;
-        if (T < 410) return -0.581 + 6.34e-3 * T - 7.93e-6 * (T * T);
-        return -0.142 + 4.12e-3 * T - 5.01e-6 * (T * T);
-    }
-    return p.kfluidm[0];
-}
-__device__ __forceinline__ double dtreaction_of(const ErebusParams &p, double T,
-                                                double phi) {
-    switch (p.reaction_rate_coeff_mode) {
-    case 1: {
-        double d = T - p.c_I;
-        return -p.log_completion_rate / (p.A_I * phi) * exp(p.b_I * (d * d));
-    }
-    case 2:
-        return -p.log_completion_rate / (p.Sxo_B * phi) *
-               pow(2.0, (p.To_B - T) / p.Tscl_B);
-    case 3:
-        return -p.log_completion_rate / (p.Sxo_B * phi) *
-               exp(p.Ea_T / p.RG * (1.0 / T - 1.0 / p.To_T));
-    default:
-        return p.dtreaction;
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -223,7 +158,7 @@ __global__ void k_sort_segments(SortPtrs S, int gr) {
 // merge scatter
 // ---------------------------------------------------------------------------
 enum MergeMode { MM_SCATTER = 0, MM_REACTION = 1, MM_MELT = 2, MM_SUBGRID_S = 3,
-                 MM_SUBGRID_T = 4 };
+                 MM_SUBGRID_T = 4, MM_VALUES = 5 };
 
 template <int GRID, int MODE>
 struct MergeFields;
@@ -309,6 +244,16 @@ struct MergeFields<GP, MM_SUBGRID_T> {
     __device__ static void load(const MP &, const double *dM, const double *dH, int m,
                                 double v[N]) {
         v[0] = dM[m]; v[1] = dH[m];
+    }
+};
+
+// per-marker values (dM) and the weight sum, for scatter_p_values
+template <>
+struct MergeFields<GP, MM_VALUES> {
+    static constexpr int N = 2;
+    __device__ static void load(const MP &, const double *dM, const double *, int m,
+                                double v[N]) {
+        v[0] = dM[m]; v[1] = 1.0;
     }
 };
 
@@ -500,6 +445,21 @@ static MergeArgs merge_args(erebus_state *s, int gr, std::initializer_list<int> 
     int k = 0;
     for (int f : sums) a.sums[k++] = s->sums[f];
     return a;
+}
+
+int scatter_p_values(erebus_state *s, const double *vals, double *sum, double *wt) {
+    if (!s->sorted_valid) {
+        int rc = build_cell_sort(s);
+        if (rc) return rc;
+    }
+    MergeArgs a = {};
+    a.start = s->sort[GP].start;
+    a.idx = s->sort[GP].idx;
+    a.dM = vals;
+    a.sums[0] = sum;
+    a.sums[1] = wt;
+    launch_merge<GP, MM_VALUES>(s, a, 0);
+    return check_cuda(s, cudaGetLastError(), "scatter_p_values");
 }
 
 // E:6376-6604

@@ -52,6 +52,9 @@ int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir
 // y = A x with the assembled (unscaled) entries
 int band_apply_unscaled(erebus_state *s, BandSystem &sys, const double *x, double *y);
 int assemble_system(erebus_state *s, int kind);
+// Hands the ELL rows just written into `sys` to its direct solver (the
+// factors are recomputed at the next solve).
+int commit_assembly(erebus_state *s, BandSystem &sys);
 // Nested-dissection multifrontal LU (mfront.cu): factor the assembled ELL
 // matrix of `sys`, solve in place, release the factor storage.
 int mf_factor(erebus_state *s, BandSystem &sys, bool fp32);

@@ -140,6 +140,9 @@ struct erebus_state {
     erebus::DevScalars *hsc = nullptr;    // pinned host mirror
 
     erebus::BandSystem hydro, thermal, gravity;
+    erebus::BandSystem heat_adjoint;    // transposed heat system (adjoint.cu)
+    double *adj_mem = nullptr;          // adjoint tape and work arrays
+    size_t adj_cap = 0;
     bool sorted_valid = false;
     double last_maxDT = 0.0;     // max|DT| of the last heat solve
 
@@ -179,4 +182,7 @@ int nodes_to_markers(erebus_state *s, double dt, int timestep);
 int advect(erebus_state *s, double dt);
 int replenish(erebus_state *s, int timestep, int64_t *marknum);
 int build_cell_sort(erebus_state *s);
+// P-node sums of w * vals[m] over the markers in marker order (the scatter of
+// marker_to_p_nodes!, E:1814-1863), and of the weights, without normalising.
+int scatter_p_values(erebus_state *s, const double *vals, double *sum, double *wt);
 }  // namespace erebus

@@ -11,7 +11,8 @@ import os
 
 import numpy as np
 
-from .abi import (STATUS_NAMES, ErebusFactorStats, ErebusGridHost, ErebusMarkersHost,
+from .abi import (STATUS_NAMES, ErebusAdjointStats, ErebusFactorStats, ErebusGridHost,
+                  ErebusMarkersHost,
                   ErebusParams, ErebusSolverOptions, ErebusSolveStats, ErebusStepStats,
                   ErebusSumsHost)
 
@@ -27,7 +28,7 @@ EXPORTS = [
     "erebus_hydromech_pass", "erebus_thermal_solve", "erebus_nodes_to_markers",
     "erebus_advect_rk4", "erebus_replenish", "erebus_step", "erebus_export_hydromech",
     "erebus_apply_hydromech", "erebus_kernel_launches", "erebus_factor_stats",
-    "erebus_snapshot_begin", "erebus_snapshot_wait",
+    "erebus_snapshot_begin", "erebus_snapshot_wait", "erebus_adjoint_heat",
 ]
 
 
@@ -70,6 +71,8 @@ def load_library(path=LIB_PATH):
         "erebus_snapshot_begin": [P, ctypes.POINTER(ErebusGridHost),
                                   ctypes.POINTER(ErebusMarkersHost)],
         "erebus_snapshot_wait": [P, pI64, pD, pD],
+        "erebus_adjoint_heat": [P, I32, I32, I32, pD, pD, pD,
+                                ctypes.POINTER(ErebusAdjointStats)],
         "erebus_set_time": [P, D, D],
         "erebus_get_time": [P, pD, pD],
         "erebus_markers_to_nodes": [P, D],
@@ -110,6 +113,7 @@ class Simulation:
         self.host = host
         self.p = host.p
         cap = int(capacity or host.capacity)
+        self.capacity = cap
         h = ctypes.c_void_p()
         self._check("erebus_create", self.L.erebus_create(ctypes.byref(self.p), cap,
                                                           ctypes.byref(h)), None)
@@ -252,6 +256,21 @@ class Simulation:
         s = ErebusStepStats()
         self._check("erebus_step", self.L.erebus_step(self.h, timestep, ctypes.byref(s)))
         return s
+
+    def adjoint_heat(self, n_steps, checkpoint_every=5, first_timestep=1):
+        """Runs n_steps timesteps and returns (J, dJ/dphim, dJ/dratio_al,
+        ErebusAdjointStats): J is the mean of the 4-P-node average of tk2
+        over the basic nodes inside the body after the last step; the
+        gradients come from the reverse sweep of erebus_adjoint_heat (states
+        at mechanical rest only; see include/erebus_b200.h)."""
+        J, dr = ctypes.c_double(), ctypes.c_double()
+        st = ErebusAdjointStats()
+        g = np.zeros(self.capacity)
+        self._check("erebus_adjoint_heat", self.L.erebus_adjoint_heat(
+            self.h, first_timestep, n_steps, checkpoint_every, ctypes.byref(J),
+            g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(dr),
+            ctypes.byref(st)))
+        return J.value, g[: st.markers].copy(), dr.value, st
 
     def export_hydromech(self, dt):
         """The assembled Stokes-Darcy system as COO (rows, cols, vals) and R."""

@@ -211,6 +211,17 @@ typedef struct ErebusFactorStats {
     double  solve_bytes;       /* per solve */
 } ErebusFactorStats;
 
+/* Statistics of one erebus_adjoint_heat call. */
+typedef struct ErebusAdjointStats {
+    int32_t steps;             /* timesteps run forward and reversed */
+    int32_t checkpoints;       /* marker-temperature checkpoints stored */
+    int32_t adjoint_solves;    /* triangular solves of the transposed heat systems */
+    int32_t factorizations;    /* factorisations of the transposed heat systems */
+    int64_t markers;           /* entries written to dJ_dphim */
+    double  J;                 /* objective after the last timestep [K] */
+    double  body_nodes;        /* basic nodes inside the body (J's average) */
+} ErebusAdjointStats;
+
 typedef struct erebus_state erebus_state;
 
 /* ---- parameters --------------------------------------------------------- */
@@ -298,6 +309,33 @@ int erebus_replenish(erebus_state *s, int32_t timestep, int64_t *marknum);
    with the thermochemical and plastic iteration loops).  Updates the
    state's dt and timesum. */
 int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st);
+
+/* ---- adjoint of the heat path (no reference counterpart) ----------------
+   Runs n_steps timesteps forward from the current state (erebus_step with
+   timesteps first_timestep, first_timestep+1, ...), evaluates
+       J = mean over the basic nodes inside the body (distance from the centre
+           < rplanet) of the 4-P-node average of tk2 after the last step
+   and returns dJ/d(phim[m]) for the markers present at the call and
+   dJ/d(ratio_al), by reverse-mode differentiation: transposed heat solves
+   (assembled from the tape of each step's RHOCP, KX, KY, dt), the transposed
+   node normalisations and marker scatters (gathers), the transposed
+   temperature gather (a marker-order scatter) and the derivatives of the
+   marker laws (E:700-750, E:1116-1357, E:2272-2358).  Marker temperatures are
+   checkpointed every `checkpoint_every` steps and recomputed in between from
+   the per-step node temperatures.
+
+   Scope: states at mechanical rest -- self-gravity G = 0, no boundary
+   strain rate, reactions off, no subgrid diffusion, zero marker stresses --
+   in which velocities, porosity change and marker motion vanish, so the heat
+   path is the whole first-order dependence of J on phim and ratio_al.  Other
+   states return EREBUS_EINVAL before running; a forward run in which a
+   time-step limiter acts, a second thermochemical iteration is taken, a
+   marker moves or the marker count changes returns EREBUS_EINVAL after it
+   (the state has then advanced).  dJ_dphim (marknum entries) and
+   dJ_dratio_al may be NULL. */
+int erebus_adjoint_heat(erebus_state *s, int32_t first_timestep, int32_t n_steps,
+                        int32_t checkpoint_every, double *J, double *dJ_dphim,
+                        double *dJ_dratio_al, ErebusAdjointStats *st);
 
 /* ---- debugging / parity ----------------------------------------------- */
 /* Runs recompute_bulk_viscosity! (E:3634), then assembles the Stokes-Darcy
