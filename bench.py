@@ -10,6 +10,10 @@ rank's device time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--workload planetesimal_401] [--direct-solver band]
+
+The line also carries "adjoint": gradients per second of the heat-path
+adjoint (20 timesteps forward and reversed, checkpoints every 5) on the
+141x141 adjoint workload at mechanical rest.
 """
 import argparse
 import json
@@ -244,6 +248,56 @@ def algorithmic_bytes(st):
     }
 
 
+def measure_adjoint(pkg, world, reps=3, n_steps=20, every=5):
+    """Gradients per second of erebus_adjoint_heat on the 141x141 adjoint
+    workload (4x4 markers per cell, porosity U(0.05, 0.25)) at mechanical
+    rest: each gradient is n_steps timesteps forward plus the reverse sweep,
+    from the same initial state (re-uploaded, untimed)."""
+    import torch
+    from erebus_b200.adjoint import at_rest
+    name = "planetesimal_141_adjoint"
+    st = at_rest(pkg.make_state(name))
+    sim = pkg.Simulation(st)
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    sim.adjoint_heat(n_steps, every)          # warm-up: plans and tape
+    sim.upload()
+    e0, e1 = ev(), ev()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for ts in range(1, n_steps + 1):
+        sim.step(ts)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    times = []
+    for _ in range(reps):
+        sim.upload()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        J, g, gr, ast = sim.adjoint_heat(n_steps, every)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    sim.close()
+    ms = max_over_ranks(sum(times) / reps, world)
+    return {"metric": "adjoint grads/sec", "value": world * 1000.0 / ms,
+            "unit": "gradients/s", "ms_per_gradient": ms,
+            "forward_ms": fwd_ms, "reverse_overhead": ms / fwd_ms,
+            "gradients": reps,
+            "J": J, "dJ_dratio_al": gr, "max_abs_dJ_dphim": float(np.abs(g).max()),
+            "adjoint_solves": ast.adjoint_solves,
+            "config": {"workload": name, "grid": "141x141 basic nodes",
+                       "markers": int(ast.markers), "markers_per_cell": "4x4",
+                       "timesteps": n_steps, "checkpoint_every": every,
+                       "objective": "mean basic-node temperature inside the body after the "
+                                    "last timestep",
+                       "parameters": "per-marker porosity and the 26Al/27Al ratio",
+                       "state": "mechanical rest: G = 0, reactions off (the adjoint's scope)"}}
+
+
 def run_ours(args):
     rank, world, local = dist_setup(args.gpus)
     import torch
@@ -305,6 +359,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
     sim2.close()
+    adj = None if args.no_adjoint else measure_adjoint(pkg, world)
     e2e = {"value": world * ne2e / (e2e_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
            "steps": ne2e}
@@ -363,7 +418,8 @@ def run_ours(args):
                                            k: v.fp64_refactorizations
                                            for k, v in fstats.items()}}),
                 "roofline": roof, "roofline_solve": roof_solve, "phases": per,
-                "cpu_baseline": cpu, "clocks": ck, "e2e": e2e, "gpu_launches": launches}
+                "cpu_baseline": cpu, "clocks": ck, "e2e": e2e, "gpu_launches": launches,
+                "adjoint": adj}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -378,6 +434,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint gradients/s measurement")
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=["planetesimal_41", "planetesimal_141", "planetesimal_401"])
     ap.add_argument("--direct-solver", default="multifrontal", choices=["multifrontal", "band"])

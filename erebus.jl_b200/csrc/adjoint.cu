@@ -119,10 +119,12 @@ __global__ void k_adj_replay(Geo g, const double *xm, const double *ym, int n,
 
 // Row r of the transposed heat matrix (column r of assemble_thermal_lse!'s
 // matrix, E:4526-4611), row-scaled, with right-hand side
-// seed_scale * seed + S.  Entries in column order.
+// seed_scale * seed + S.  Entries in column order.  Any scaled entry that
+// differs from the last factorised matrix (prev) sets *changed.
 __global__ void k_adj_assemble(Geo g, const double *rhocp, const double *KX,
                                const double *KY, double dt, const double *seed,
-                               double seed_scale, const double *S, BandView B) {
+                               double seed_scale, const double *S, BandView B,
+                               const double *prev, int *changed) {
     int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= B.NB * (int64_t)B.nb) return;
     int col[5];
@@ -177,10 +179,14 @@ __global__ void k_adj_assemble(Geo g, const double *rhocp, const double *KX,
     double sc = sum > 0.0 ? 1.0 / sum : 1.0;
     B.rhs[r] = rhs * sc;
     B.rscale[r] = sc;
+    int diff = 0;
     for (int k = 0; k < B.ell; k++) {
+        double v = k < ne ? val[k] * sc : 0.0;
         B.ell_cols[r * B.ell + k] = k < ne ? col[k] : -1;
-        B.ell_vals[r * B.ell + k] = k < ne ? val[k] * sc : 0.0;
+        B.ell_vals[r * B.ell + k] = v;
+        diff |= __double_as_longlong(prev[r * B.ell + k]) != __double_as_longlong(v);
     }
+    if (diff) atomicOr(changed, 1);
 }
 
 struct AdjNodeIn {
@@ -489,10 +495,17 @@ extern "C" int erebus_adjoint_heat(erebus_state *s, int32_t first_timestep, int3
             const bool last = q == N - 1;
             const size_t o = (size_t)q * np;
             if (!last) ATRY(scatter_p_values(s, L.Tbar, L.S, L.Swt));
+            // the factors of the previous (later) step are kept when the
+            // transposed matrix is bitwise the same
+            ATRY(check_cuda(s, cudaMemsetAsync(A.changed, 0, sizeof(int), s->stream),
+                            "adjoint"));
             EREBUS_LAUNCH(s, k_adj_assemble, nblocks(rows, 128), 128, 0, g, L.rhocp + o,
                           L.KX + o, L.KY + o, dts[q], L.seed, last ? 1.0 : 0.0,
-                          last ? (const double *)nullptr : L.S, band_view(A));
-            ATRY(commit_assembly(s, A));
+                          last ? (const double *)nullptr : L.S, band_view(A), A.ell_prev,
+                          A.changed);
+            int changed = 1;
+            ATRY(read_flag(s, A.changed, &changed));
+            if (changed || !A.factored || !s->opt.reuse_factors) ATRY(commit_assembly(s, A));
             ErebusSolveStats ss = {};
             ATRY(band_solve_refined(s, A, s->opt.thermal_rtol, s->opt.max_refinements, &ss));
             solves += ss.iterations;
