@@ -152,13 +152,20 @@ def dist_setup(n):
 
 
 def max_over_ranks(x, world):
+    """The largest of the ranks' values (device times): the job's time."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(units_per_rank, ms_per_rank, world):
+    """Whole-job throughput: all ranks' units over the slowest rank's time."""
+    return world * units_per_rank / (max_over_ranks(ms_per_rank, world) / 1000.0)
 
 
 def barrier(world):
