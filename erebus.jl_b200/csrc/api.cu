@@ -227,8 +227,22 @@ int erebus_destroy(erebus_state *s) {
     }
     if (s->snap_dev) cudaFree(s->snap_dev);
     if (s->snap_tm) cudaFreeHost(s->snap_tm);
+    if (s->tm64) cudaFree(s->tm64);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
+    return EREBUS_OK;
+}
+
+int erebus_grid_layout(const ErebusParams *p, int64_t *offsets, int64_t *total_bytes) {
+    if (!p || !offsets || p->Nx < 2 || p->Ny < 2) return EREBUS_EINVAL;
+    int64_t nb = (int64_t)p->Nx * p->Ny, np = (int64_t)(p->Nx + 1) * (p->Ny + 1), o = 0;
+    for (int f = 0; f < G_COUNT; f++) {
+        int64_t n = is_basic_field(f) ? nb : np;
+        int64_t b = is_bool_field(f) ? n : n * 8;
+        offsets[f] = o;
+        o += (b + 255) / 256 * 256;
+    }
+    if (total_bytes) *total_bytes = o;
     return EREBUS_OK;
 }
 
@@ -272,11 +286,14 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
     }
     s->tm8 = (int8_t *)alloc(cap);
     if (!s->tm8) return fail(EREBUS_ENOMEM, "markers");
-    for (int f = 0; f < G_COUNT; f++) {
-        size_t n = is_basic_field(f) ? nbn : np;
-        s->grid[f] = (double *)alloc(is_bool_field(f) ? n : n * 8);
-        if (!s->grid[f]) return fail(EREBUS_ENOMEM, "grid");
+    {   // one slab in the layout of erebus_grid_layout
+        int64_t off[G_COUNT], total = 0;
+        erebus_grid_layout(p, off, &total);
+        char *slab = (char *)alloc((size_t)total);
+        if (!slab) return fail(EREBUS_ENOMEM, "grid");
+        for (int f = 0; f < G_COUNT; f++) s->grid[f] = (double *)(slab + off[f]);
     }
+    (void)nbn;
     for (int f = 0; f < S_COUNT; f++) {
         s->sums[f] = (double *)alloc((is_basic_sum(f) ? nbn : np) * 8);
         if (!s->sums[f]) return fail(EREBUS_ENOMEM, "sums");
@@ -473,6 +490,7 @@ int erebus_snapshot_begin(erebus_state *s, const ErebusGridHost *gh,
     if (s->snap_cap < need) {
         if (s->snap_dev) cudaFree(s->snap_dev);
         if (s->snap_tm) cudaFreeHost(s->snap_tm);
+    if (s->tm64) cudaFree(s->tm64);
         s->snap_dev = nullptr;
         s->snap_tm = nullptr;
         s->snap_cap = 0;
@@ -710,10 +728,11 @@ int erebus_replenish(erebus_state *s, int32_t timestep, int64_t *marknum) {
     return replenish(s, timestep, marknum);
 }
 
-// One timestep (E:6370-7235).
-int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st) {
-    if (!s || timestep < 1) return EREBUS_EINVAL;
-    cudaSetDevice(s->device);
+// One timestep (E:6370-7235).  `after_m2n` (may be NULL) is called once the
+// markers->nodes phase is enqueued.
+typedef int (*StepHook)(erebus_state *s, void *ctx);
+static int step_impl(erebus_state *s, int32_t timestep, ErebusStepStats *st,
+                     StepHook after_m2n, void *ctx) {
     const ErebusParams &p = s->p;
     ErebusStepStats stats = {};
     double worst = 0.0;
@@ -721,6 +740,7 @@ int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st) {
     timer_begin(s, PH_MARKERS_TO_NODES);
     TRY(markers_to_nodes(s, s->timesum));
     timer_end(s, PH_MARKERS_TO_NODES);
+    if (after_m2n) TRY(after_m2n(s, ctx));
     ErebusSolveStats gs = {};
     timer_begin(s, PH_GRAVITY);
     TRY(erebus_gravity(s, &gs));
@@ -776,6 +796,178 @@ int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st) {
     stats.timesum = s->timesum;
     stats.worst_rel_residual = worst;
     stats.factorizations = (s->hydro.factorizations - hydro_f0) * 1000 + (s->thermal.factorizations - th_f0);
+    if (st) *st = stats;
+    return EREBUS_OK;
+}
+
+int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st) {
+    if (!s || timestep < 1) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    return step_impl(s, timestep, st, nullptr, nullptr);
+}
+
+// ---- one timestep on host arrays --------------------------------------------
+// Marker fields the timestep does not change for the markers it starts with
+// (replenishment only appends): the material constants, and the derived
+// properties once compute_marker_properties! (E:700-750) has run.  They are
+// copied back while the rest of the timestep runs.
+static const int kEarlyFields[] = {
+    M_rhototalm, M_rhocptotalm, M_etatotalm, M_hrtotalm, M_ktotalm, M_tkm_rhocptotalm,
+    M_etafluidcur_inv_kphim, M_inv_gggtotalm, M_fricttotalm, M_cohestotalm, M_tenstotalm,
+    M_rhofluidcur, M_alphasolidcur, M_alphafluidcur, M_etasolidm_m};
+
+static bool is_early(int f) {
+    for (int e : kEarlyFields)
+        if (e == f) return true;
+    return false;
+}
+
+__global__ void k_tm_narrow(const int64_t *tm, int8_t *tm8, int64_t n, int *err) {
+    int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    int64_t t = tm[m];
+    if (t < 1 || t > 3) {
+        atomicExch(err, 1);
+        t = 3;
+    }
+    tm8[m] = (int8_t)t;
+}
+__global__ void k_tm_widen(const int8_t *tm8, int64_t *tm, int64_t b, int64_t e) {
+    int64_t m = b + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < e) tm[m] = tm8[m];
+}
+
+// Copies the grid between the device slab and host arrays: one copy when the
+// host arrays sit at the offsets of erebus_grid_layout from the first one,
+// else one per field.
+static int copy_grid(erebus_state *s, double *dev, const void *const *host,
+                     cudaMemcpyKind kind) {
+    int64_t off[G_COUNT], total = 0;
+    erebus_grid_layout(&s->p, off, &total);
+    const char *h0 = (const char *)host[0];
+    bool slab = true;
+    for (int f = 0; f < G_COUNT && slab; f++) slab = (const char *)host[f] == h0 + off[f];
+    if (slab) {
+        void *d = kind == cudaMemcpyHostToDevice ? (void *)dev : (void *)h0;
+        const void *src = kind == cudaMemcpyHostToDevice ? (const void *)h0 : (const void *)dev;
+        return check_cuda(s, cudaMemcpyAsync(d, src, (size_t)total, kind, s->stream), "grid copy");
+    }
+    for (int f = 0; f < G_COUNT; f++) {
+        char *d = (char *)dev + off[f];
+        int rc = kind == cudaMemcpyHostToDevice
+                     ? check_cuda(s, cudaMemcpyAsync(d, host[f], field_bytes(s, f), kind,
+                                                     s->stream), "grid copy")
+                     : check_cuda(s, cudaMemcpyAsync((void *)host[f], d, field_bytes(s, f), kind,
+                                                     s->stream), "grid copy");
+        if (rc) return rc;
+    }
+    return EREBUS_OK;
+}
+
+struct HostStepCtx {
+    ErebusMarkersHost *out;
+    int64_t n;
+};
+
+static int early_copies(erebus_state *s, void *vctx) {
+    HostStepCtx &c = *static_cast<HostStepCtx *>(vctx);
+    void *const *dst = reinterpret_cast<void *const *>(c.out);
+    TRY(check_cuda(s, cudaEventRecord(s->snap_ready, s->stream), "step_host"));
+    TRY(check_cuda(s, cudaStreamWaitEvent(s->copy_stream, s->snap_ready, 0), "step_host"));
+    if (c.n == 0) return EREBUS_OK;
+    for (int f : kEarlyFields)
+        if (dst[f])
+            TRY(check_cuda(s, cudaMemcpyAsync(dst[f], s->m[f], c.n * 8, cudaMemcpyDeviceToHost,
+                                              s->copy_stream), "step_host"));
+    // tm of these markers is what was uploaded
+    return check_cuda(s, cudaMemcpyAsync(c.out->tm, s->tm64, c.n * 8, cudaMemcpyDeviceToHost,
+                                         s->copy_stream), "step_host");
+}
+
+int erebus_step_host(erebus_state *s, int32_t timestep, const ErebusMarkersHost *in,
+                     int64_t marknum, const ErebusGridHost *gin, ErebusMarkersHost *out,
+                     int64_t *marknum_out, ErebusGridHost *gout, ErebusStepStats *st) {
+    if (!s || timestep < 1 || !in || !gin || !out || !gout || marknum < 0 ||
+        marknum > s->capacity)
+        return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    const void *const *src = reinterpret_cast<const void *const *>(in);
+    void *const *dst = reinterpret_cast<void *const *>(out);
+    const void *const *gsrc = reinterpret_cast<const void *const *>(gin);
+    void *const *gdst = reinterpret_cast<void *const *>(gout);
+    for (int f = 0; f < M_COUNT; f++) {
+        bool optional = f == M_etasolidm_m && !s->p.per_marker_eta;
+        if ((!src[f] || !dst[f]) && !optional) return EREBUS_EINVAL;
+    }
+    for (int f = 0; f < G_COUNT; f++)
+        if (!gsrc[f] || !gdst[f]) return EREBUS_EINVAL;
+    if (!s->copy_stream) {
+        if (cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->snap_ready, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->snap_done, cudaEventDisableTiming) != cudaSuccess) {
+            s->last_error = "step_host: stream or event creation failed";
+            return EREBUS_ECUDA;
+        }
+    }
+    if (s->snap_pending) return EREBUS_EINVAL;   // the copy stream is busy
+    if (!s->tm64 && cudaMalloc(&s->tm64, (size_t)s->capacity * 8) != cudaSuccess) {
+        s->tm64 = nullptr;
+        s->last_error = "step_host: scratch allocation failed";
+        return EREBUS_ENOMEM;
+    }
+    // host -> device: markers (tm widened to int64 on the host side, narrowed
+    // and checked on the device) and the grid
+    for (int f = 0; f < M_COUNT; f++) {
+        if (f == M_tm || !src[f] || marknum == 0) continue;
+        TRY(check_cuda(s, cudaMemcpyAsync(s->m[f], src[f], marknum * 8,
+                                          cudaMemcpyHostToDevice, s->stream), "step_host"));
+    }
+    if (marknum > 0)
+        TRY(check_cuda(s, cudaMemcpyAsync(s->tm64, in->tm, marknum * 8, cudaMemcpyHostToDevice,
+                                          s->stream), "step_host"));
+    TRY(copy_grid(s, s->grid[0], gsrc, cudaMemcpyHostToDevice));
+    TRY(check_cuda(s, cudaMemsetAsync(&s->dsc->err, 0, sizeof(int), s->stream), "step_host"));
+    if (marknum > 0)
+        EREBUS_LAUNCH(s, k_tm_narrow, nblocks(marknum), kThreads, 0, s->tm64, s->tm8, marknum,
+                      &s->dsc->err);
+    int bad = 0;
+    TRY(check_cuda(s, cudaMemcpyAsync(&bad, &s->dsc->err, sizeof(int), cudaMemcpyDeviceToHost,
+                                      s->stream), "step_host"));
+    TRY(check_cuda(s, cudaStreamSynchronize(s->stream), "step_host"));
+    if (bad) {
+        s->last_error = "step_host: marker type outside 1..3";
+        return EREBUS_EINVAL;
+    }
+    s->marknum = marknum;
+    s->sorted_valid = false;
+    // the timestep, with the early copies on the copy stream
+    HostStepCtx ctx = {out, marknum};
+    ErebusStepStats stats = {};
+    int rc = step_impl(s, timestep, &stats, early_copies, &ctx);
+    if (rc) {
+        cudaStreamSynchronize(s->copy_stream);
+        return rc;
+    }
+    // device -> host: the rest
+    const int64_t n2 = s->marknum;
+    for (int f = 0; f < M_COUNT; f++) {
+        if (f == M_tm || !dst[f]) continue;
+        int64_t b = is_early(f) ? marknum : 0;
+        if (n2 > b)
+            TRY(check_cuda(s, cudaMemcpyAsync((double *)dst[f] + b, s->m[f] + b, (n2 - b) * 8,
+                                              cudaMemcpyDeviceToHost, s->stream), "step_host"));
+    }
+    if (n2 > marknum) {
+        EREBUS_LAUNCH(s, k_tm_widen, nblocks(n2 - marknum), kThreads, 0, s->tm8, s->tm64,
+                      marknum, n2);
+        TRY(check_cuda(s, cudaMemcpyAsync(out->tm + marknum, s->tm64 + marknum,
+                                          (n2 - marknum) * 8, cudaMemcpyDeviceToHost, s->stream),
+                       "step_host"));
+    }
+    TRY(copy_grid(s, s->grid[0], (const void *const *)gdst, cudaMemcpyDeviceToHost));
+    TRY(check_cuda(s, cudaStreamSynchronize(s->copy_stream), "step_host"));
+    TRY(check_cuda(s, cudaStreamSynchronize(s->stream), "step_host"));
+    if (marknum_out) *marknum_out = n2;
     if (st) *st = stats;
     return EREBUS_OK;
 }

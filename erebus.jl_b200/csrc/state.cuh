@@ -130,6 +130,7 @@ struct erebus_state {
     int64_t snap_marknum = 0;
     double snap_dt = 0.0, snap_timesum = 0.0;
     int64_t *snap_tm_dst = nullptr;
+    int64_t *tm64 = nullptr;                   // int64 marker types (erebus_step_host)
     double *partials = nullptr;                // reduction partials
     // replenishment scratch (per marker-grid anchor)
     unsigned long long *a_mdis = nullptr;

@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "liberebus_b200.so")
 EXPORTS = [
     "erebus_default_params", "erebus_default_solver_options", "erebus_check_params",
     "erebus_create", "erebus_destroy", "erebus_set_solver_options", "erebus_last_error",
+    "erebus_grid_layout",
     "erebus_upload_markers", "erebus_download_markers", "erebus_upload_grid",
     "erebus_download_grid", "erebus_download_sums", "erebus_set_time", "erebus_get_time",
     "erebus_markers_to_nodes", "erebus_gravity", "erebus_thermochemical_reaction",
@@ -29,6 +30,7 @@ EXPORTS = [
     "erebus_advect_rk4", "erebus_replenish", "erebus_step", "erebus_export_hydromech",
     "erebus_apply_hydromech", "erebus_kernel_launches", "erebus_factor_stats",
     "erebus_snapshot_begin", "erebus_snapshot_wait", "erebus_adjoint_heat",
+    "erebus_step_host",
 ]
 
 
@@ -60,6 +62,7 @@ def load_library(path=LIB_PATH):
         "erebus_default_solver_options": [ctypes.POINTER(ErebusSolverOptions)],
         "erebus_check_params": [ctypes.POINTER(ErebusParams)],
         "erebus_create": [ctypes.POINTER(ErebusParams), I64, PP],
+        "erebus_grid_layout": [ctypes.POINTER(ErebusParams), pI64, pI64],
         "erebus_destroy": [P],
         "erebus_set_solver_options": [P, ctypes.POINTER(ErebusSolverOptions)],
         "erebus_factor_stats": [P, I32, ctypes.POINTER(ErebusFactorStats)],
@@ -73,6 +76,10 @@ def load_library(path=LIB_PATH):
         "erebus_snapshot_wait": [P, pI64, pD, pD],
         "erebus_adjoint_heat": [P, I32, I32, I32, pD, pD, pD,
                                 ctypes.POINTER(ErebusAdjointStats)],
+        "erebus_step_host": [P, I32, ctypes.POINTER(ErebusMarkersHost), I64,
+                             ctypes.POINTER(ErebusGridHost), ctypes.POINTER(ErebusMarkersHost),
+                             pI64, ctypes.POINTER(ErebusGridHost),
+                             ctypes.POINTER(ErebusStepStats)],
         "erebus_set_time": [P, D, D],
         "erebus_get_time": [P, pD, pD],
         "erebus_markers_to_nodes": [P, D],
@@ -255,6 +262,26 @@ class Simulation:
         """One whole timestep (E:6370-7235); returns ErebusStepStats."""
         s = ErebusStepStats()
         self._check("erebus_step", self.L.erebus_step(self.h, timestep, ctypes.byref(s)))
+        return s
+
+    def step_host(self, timestep):
+        """One timestep on the HostState's arrays (erebus_step_host): they
+        are uploaded, advanced and copied back in one call; returns
+        ErebusStepStats and updates marknum, dt and timesum of the host."""
+        h = self.host
+        # the ctypes views are rebuilt only when an array object changed
+        key = tuple(id(a) for a in h.m.values()) + tuple(id(a) for a in h.grid.values())
+        if getattr(self, "_views_key", None) != key:
+            self._views = (h.markers_struct(), h.grid_struct())
+            self._views_key = key
+        ms, gs = self._views
+        n = ctypes.c_int64()
+        s = ErebusStepStats()
+        self._check("erebus_step_host", self.L.erebus_step_host(
+            self.h, timestep, ctypes.byref(ms), h.marknum, ctypes.byref(gs), ctypes.byref(ms),
+            ctypes.byref(n), ctypes.byref(gs), ctypes.byref(s)))
+        h.marknum = n.value
+        h.dt, h.timesum = s.dt, s.timesum
         return s
 
     def adjoint_heat(self, n_steps, checkpoint_every=5, first_timestep=1):

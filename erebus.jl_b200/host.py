@@ -55,6 +55,21 @@ def u01(seed, stream, idx):
     return (z >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
 
 
+def grid_layout(p):
+    """Byte offsets of the grid arrays in one block, and the block size: each
+    array at the next multiple of 256 bytes after the previous one (the
+    layout of erebus_grid_layout, in which erebus_step_host copies the grid in
+    one transfer)."""
+    nb, npn = p.Nx * p.Ny, (p.Nx + 1) * (p.Ny + 1)
+    off, o = {}, 0
+    for name in GRID_FIELDS:
+        n = nb if name in BASIC_GRID else npn
+        b = n if name in BOOL_GRID else 8 * n
+        off[name] = o
+        o += (b + 255) // 256 * 256
+    return off, o
+
+
 class HostState:
     """Numpy arrays for one planetesimal, plus ctypes views of them.
 
@@ -75,17 +90,46 @@ class HostState:
         for name in MARKER_FIELDS:
             dt = np.int64 if name == "tm" else np.float64
             self.m[name] = zeros(self.capacity, dt)
-        self.grid = {}
-        for name in GRID_FIELDS:
-            shape = (g.Ny, g.Nx) if name in BASIC_GRID else (g.Ny1, g.Nx1)
-            dt = np.uint8 if name in BOOL_GRID else np.float64
-            self.grid[name] = zeros(shape, dt, order="F")
+        self.grid = self._grid_block(pinned)
         self.sums = {}
         for name in SUM_FIELDS:
             shape = (g.Ny, g.Nx) if name in BASIC_SUMS else (g.Ny1, g.Nx1)
             self.sums[name] = np.zeros(shape, dtype=np.float64, order="F")
         self.dt = p.dt_longest          # setup_dynamic_simulation_parameters
         self.timesum = p.start_time     # (E:55-70)
+
+    def _grid_block(self, pinned):
+        """Grid arrays as views of one zeroed block in the grid_layout."""
+        g = self.g
+        off, total = grid_layout(self.p)
+        if pinned:
+            import torch
+            t = torch.zeros(total, dtype=torch.uint8, pin_memory=True)
+            self._pins.append(t)
+            block = t.numpy()
+        else:
+            block = np.zeros(total, dtype=np.uint8)
+        grid = {}
+        for name in GRID_FIELDS:
+            shape = (g.Ny, g.Nx) if name in BASIC_GRID else (g.Ny1, g.Nx1)
+            dt = np.dtype(np.uint8 if name in BOOL_GRID else np.float64)
+            n = shape[0] * shape[1]
+            grid[name] = block[off[name]: off[name] + n * dt.itemsize].view(dt).reshape(
+                shape, order="F")
+        return grid
+
+    def pinned(self):
+        """A copy of this state in page-locked host memory (grid in one
+        block), for asynchronous transfers."""
+        o = HostState(self.p, self.capacity, pinned=True)
+        for k, v in self.m.items():
+            o.m[k][...] = v
+        for k, v in self.grid.items():
+            o.grid[k][...] = v
+        for k, v in self.sums.items():
+            o.sums[k][...] = v
+        o.marknum, o.dt, o.timesum = self.marknum, self.dt, self.timesum
+        return o
 
     def _pinned_zeros(self, shape, dtype, order="C"):
         import torch

@@ -235,6 +235,12 @@ int erebus_check_params(const ErebusParams *p);
 /* ---- lifecycle (replaces the setup_* allocators E:55-592, E:851, E:2976) */
 int erebus_create(const ErebusParams *p, int64_t marker_capacity,
                   erebus_state **out);
+/* Byte offsets of the grid arrays (ErebusGridHost order) in one block of
+   *total_bytes: each array follows the previous one at the next multiple of
+   256 bytes.  The device keeps its grid in this layout; host grid arrays
+   placed at these offsets from the first one are copied in one transfer by
+   erebus_step_host (else one transfer per array). */
+int erebus_grid_layout(const ErebusParams *p, int64_t *offsets, int64_t *total_bytes);
 int erebus_destroy(erebus_state *s);
 int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o);
 /* Sizes and work of the direct solver of `system` (EREBUS_SYSTEM_*). */
@@ -309,6 +315,20 @@ int erebus_replenish(erebus_state *s, int32_t timestep, int64_t *marknum);
    with the thermochemical and plastic iteration loops).  Updates the
    state's dt and timesum. */
 int erebus_step(erebus_state *s, int32_t timestep, ErebusStepStats *st);
+/* The same timestep on host arrays: uploads `in` (marknum markers) and `gin`,
+   runs the timestep and copies the markers (*marknum_out after
+   replenishment) and the grid into `out` and `gout`, which may be the same
+   arrays as `in` and `gin`.  The marker fields the timestep does not change
+   for the markers it starts with (material constants, and the derived
+   properties once compute_marker_properties! has run) are copied back on a
+   second stream while the solves run, so with page-locked host arrays part
+   of the copy-out overlaps the timestep.  `out` arrays need room for the
+   state's capacity.  EREBUS_EINVAL for a NULL array (etasolidm_m may be NULL
+   unless per_marker_eta), a marker type outside 1..3 (nothing runs), or a
+   snapshot in flight. */
+int erebus_step_host(erebus_state *s, int32_t timestep, const ErebusMarkersHost *in,
+                     int64_t marknum, const ErebusGridHost *gin, ErebusMarkersHost *out,
+                     int64_t *marknum_out, ErebusGridHost *gout, ErebusStepStats *st);
 
 /* ---- adjoint of the heat path (no reference counterpart) ----------------
    Runs n_steps timesteps forward from the current state (erebus_step with

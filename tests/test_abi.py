@@ -87,3 +87,22 @@ def test_create_fails_loudly_without_device(pkg, built_lib):
     with pytest.raises(pkg.ErebusError) as e:
         pkg.Simulation(st)
     assert e.value.code == 7   # EREBUS_ENODEVICE
+
+
+def test_grid_layout_matches_library(pkg, built_lib):
+    """The host grid block (HostState) and the device slab share one layout,
+    so erebus_step_host copies the grid in one transfer."""
+    import ctypes
+
+    from erebus_b200.abi import GRID_FIELDS
+    from erebus_b200.host import grid_layout
+    p = pkg.config_params("planetesimal_141")
+    off = (ctypes.c_int64 * len(GRID_FIELDS))()
+    total = ctypes.c_int64()
+    built_lib.erebus_grid_layout.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    assert built_lib.erebus_grid_layout(ctypes.byref(p), off, ctypes.byref(total)) == 0
+    mine, tot = grid_layout(p)
+    assert [mine[k] for k in GRID_FIELDS] == list(off) and tot == total.value
+    st = pkg.HostState(p)
+    base = st.grid[GRID_FIELDS[0]].ctypes.data
+    assert all(st.grid[k].ctypes.data == base + mine[k] for k in GRID_FIELDS)

@@ -39,7 +39,7 @@ def _rank(rank, world, port, out):
 
 def test_two_gloo_ranks_time_the_job_by_the_slowest_rank():
     world, port = 2, _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.start_processes(_rank, args=(world, port, out), nprocs=world, join=True,
                            start_method="spawn")
