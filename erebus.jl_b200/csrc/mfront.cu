@@ -46,6 +46,7 @@ struct MfView {
     const int *eamap;   // local -> children's update index
     const int *lvl;     // level ranges (nlev + 1)
     const int *lvl_kt;  // max Kt per level
+    const int *lvl_mode;  // per level: MF_FACTOR_LOCAL, MF_SOLVE_LOCAL bits
     int nlev;
     const long long *target;   // ELL entry -> storage offset
     const int *expect;         // ELL column pattern the targets were built from
@@ -60,6 +61,7 @@ struct MfDevice {
     void *F64 = nullptr, *F32 = nullptr;   // front storage of each precision, on first use
     double *vec = nullptr;
     int *vars = nullptr, *eamap = nullptr, *lvl = nullptr, *lvl_kt = nullptr;
+    int *lvl_mode = nullptr;
     long long *target = nullptr;
     int *expect = nullptr;
     int nlev = 0;
@@ -224,6 +226,9 @@ __device__ void mf_update_tile(const MfView &V, const MfFront &f, int I, int J, 
 // Fronts of a level whose tile counts a CTA keeps in shared memory; levels
 // with more fronts run one front per CTA.
 constexpr int MF_KM_MAX = 256;
+// Bits of MfView::lvl_mode: the level runs one front per CTA in the factor /
+// in the solve (else cooperatively, tile tasks dealt over all CTAs).
+constexpr int MF_FACTOR_LOCAL = 1, MF_SOLVE_LOCAL = 2;
 
 struct MfFactorSmem {
     MmaSmem m;
@@ -316,7 +321,7 @@ k_mf_factor(MfView V, unsigned int *bar, int *err) {
     const int G = gridDim.x;
     for (int p = 0; p < V.nlev; p++) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
-        if (fe - fb >= G / 2 || fe - fb > MF_KM_MAX) {
+        if (V.lvl_mode[p] & MF_FACTOR_LOCAL) {
             for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
                 const MfFront f = V.fr[fi];
                 mf_factor_local<T>(V, f, FS, err);
@@ -620,7 +625,7 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
     // forward: leaves to root
     for (int p = 0; p < V.nlev; p++) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
-        const bool local = fe - fb >= G / 2 || fe - fb > MF_KM_MAX;
+        const bool local = V.lvl_mode[p] & MF_SOLVE_LOCAL;
         if (!local) mf_load_km(V, fb, fe, S.km);
         for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
             const MfFront f = V.fr[fi];
@@ -645,7 +650,7 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
     // backward: root to leaves
     for (int p = V.nlev - 1; p >= 0; p--) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
-        const bool local = fe - fb >= G / 2 || fe - fb > MF_KM_MAX;
+        const bool local = V.lvl_mode[p] & MF_SOLVE_LOCAL;
         if (!local) mf_load_km(V, fb, fe, S.km);
         auto ring_x = [&](const MfFront &f) {
             const int *var = V.vars + f.var_off;
@@ -688,6 +693,7 @@ static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
     V.eamap = D.eamap;
     V.lvl = D.lvl;
     V.lvl_kt = D.lvl_kt;
+    V.lvl_mode = D.lvl_mode;
     V.nlev = D.nlev;
     V.target = D.target;
     V.expect = D.expect;
@@ -701,8 +707,8 @@ bool mf_is_fp32(const BandSystem &sys) { return sys.mf && sys.mf->fp32; }
 void mf_release(BandSystem &sys) {
     MfDevice *D = sys.mf;
     if (!D) return;
-    void *ps[] = {D->fr, D->F64, D->F32, D->vec, D->vars, D->eamap, D->lvl, D->lvl_kt, D->target,
-                  D->expect};
+    void *ps[] = {D->fr, D->F64, D->F32, D->vec, D->vars, D->eamap, D->lvl, D->lvl_kt,
+                  D->lvl_mode, D->target, D->expect};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete D;
@@ -715,6 +721,51 @@ static cudaError_t upload(T **dst, const std::vector<T> &src, cudaStream_t st) {
     if (e == cudaSuccess && !src.empty())
         e = cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st);
     return e;
+}
+
+// CTAs of the cooperative factor and solve launches (2 per SM).
+static int mf_grid(erebus_state *s) {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    return 2 * sms;
+}
+
+// How each level is processed.  A level with at least G/2 fronts (or more
+// than fit the shared-memory table) runs one front per CTA.  Otherwise the
+// choice weighs the serial chain of one CTA doing a whole front against the
+// fixed cost of the cooperative phases (a grid barrier and a pass over the
+// level's fronts each): the factor runs a front per CTA when that front's
+// tile operations are few, the solve when its tile sweeps are short.  The
+// thresholds come from timing each phase of the 141x141 systems on a B200.
+constexpr int kLocalFactorOps = 20;   // tile operations per CTA
+constexpr int kLocalSolveTiles = 48;  // tiles streamed per CTA and sweep
+static std::vector<int> mf_level_modes(const MfPlan &P, int G) {
+    std::vector<int> mode;
+    for (size_t p = 0; p + 1 < P.level_begin.size(); p++) {
+        const int fb = P.level_begin[p], fe = P.level_begin[p + 1], F = fe - fb;
+        const int waves = (F + G - 1) / G;
+        long long ops = 0, tiles = 0;
+        for (int fi = fb; fi < fe; fi++) {
+            const MfFront &f = P.fronts[fi];
+            long long o = (f.c0 >= 0 || f.c1 >= 0 ? (long long)f.Mt * f.Mt : 0) + 2LL * f.Kt +
+                          (long long)(f.Mt - f.Kt) * (f.Mt - f.Kt) * f.Kt;
+            long long fwd = 0;
+            for (int K = 0; K < f.Kt; K++) {
+                const int e = f.Kt - K - 1, R = f.Mt - K - 1;
+                o += R + (long long)e * R + (long long)(f.Mt - f.Kt) * e;
+                fwd += R;
+            }
+            const long long bwd = (long long)f.Kt * (f.Kt + 1) / 2 + (long long)f.Kt * (f.Mt - f.Kt);
+            ops = std::max(ops, o);
+            tiles = std::max(tiles, std::max(fwd, bwd));
+        }
+        const bool forced = F >= G / 2 || F > MF_KM_MAX;
+        int m = 0;
+        if (forced || waves * ops <= kLocalFactorOps) m |= MF_FACTOR_LOCAL;
+        if (forced || waves * tiles <= kLocalSolveTiles) m |= MF_SOLVE_LOCAL;
+        mode.push_back(m);
+    }
+    return mode;
 }
 
 // Leaves of 16 nodes for the 6-unknown system (96 unknowns), 64 nodes for
@@ -757,6 +808,7 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
     if (e == cudaSuccess) e = upload(&D->eamap, P.eamap, s->stream);
     if (e == cudaSuccess) e = upload(&D->lvl, P.level_begin, s->stream);
     if (e == cudaSuccess) e = upload(&D->lvl_kt, lvl_kt, s->stream);
+    if (e == cudaSuccess) e = upload(&D->lvl_mode, mf_level_modes(P, mf_grid(s)), s->stream);
     if (e == cudaSuccess) e = upload(&D->target, target, s->stream);
     if (e == cudaSuccess) e = upload(&D->expect, expect, s->stream);
     if (e == cudaSuccess) e = cudaMalloc(&D->vec, P.vec * sizeof(double));
