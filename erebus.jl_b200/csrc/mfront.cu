@@ -288,18 +288,21 @@ __device__ void mf_factor_local(const MfView &V, const MfFront &f, MfFactorSmem 
 template <class Count, class Task>
 __device__ void mf_for_tasks(const MfView &V, int fb, int fe, const int2 *km, Count count,
                              Task task) {
-    const int G = gridDim.x, me = blockIdx.x;
-    long long base = 0;
+    const int G = gridDim.x;
+    // first = (blockIdx.x - tasks of the earlier fronts) mod G, kept in 32
+    // bits and updated per front: every thread runs this loop over all the
+    // level's fronts, so it must stay a few instructions per front
+    int first = blockIdx.x;
     for (int fi = fb; fi < fe; fi++) {
         int2 q = km[fi - fb];
         int cnt = count(q.x, q.y);
         if (cnt <= 0) continue;
-        int first = (int)(((me - base) % G + G) % G);
         if (first < cnt) {
             const MfFront f = V.fr[fi];
             for (int u = first; u < cnt; u += G) task(f, u);
         }
-        base += cnt;
+        first -= cnt;
+        if (first < 0) first = first % G + (first % G < 0 ? G : 0);
     }
 }
 
