@@ -293,6 +293,52 @@ def measure_adjoint(pkg, world, reps=3, n_steps=20, every=5):
                        "state": "mechanical rest: G = 0, reactions off (the adjoint's scope)"}}
 
 
+def measure_ensemble(pkg, world, rank, bodies, steps, warmup, wave):
+    """Aggregate timesteps/s of an ensemble of planetesimals of uneven sizes
+    (erebus_b200.ensemble: radius U(20, 100) km, grid side 61-201, per-body
+    porosity, 26Al/27Al and viscosity), advanced `wave` bodies at a time,
+    each body on its own host thread and stream.  Per wave: `warmup` untimed
+    timesteps, then `steps` timed ones; the time of a wave is from an event
+    before its first timed step to the last body's end event."""
+    import torch
+    from erebus_b200.ensemble import Ensemble, ensemble_states
+    done, ms_total, sides = 0, 0.0, []
+    for w0 in range(0, bodies, wave):
+        nb = min(wave, bodies - w0)
+        states = ensemble_states(nb, seed=42 + 1000 * rank, first=w0)
+        sides += [st.p.Nx for st in states]
+        ens = Ensemble(states)
+        try:
+            ens.run(warmup)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.cuda.synchronize()
+            ens.run(steps, start_step=warmup + 1)
+            ends = []
+            for h in ens.streams():
+                e = torch.cuda.Event(enable_timing=True)
+                e.record(torch.cuda.ExternalStream(h))
+                ends.append(e)
+            torch.cuda.synchronize()
+            ms_total += max(e0.elapsed_time(e) for e in ends)
+            done += nb * steps
+        finally:
+            ens.close()
+    ms = max_over_ranks(ms_total, world)
+    return {"metric": "ensemble timesteps/sec (aggregate over bodies)",
+            "value": world * done / (ms / 1000.0), "unit": "timesteps/s",
+            "bodies": bodies * world, "steps_per_body": steps, "warmup": warmup,
+            "ms": ms, "wave": wave, "grid_sides": [min(sides), max(sides)],
+            "config": {"workload": "ensemble", "radius_km": [20, 100],
+                       "grid_side": "61-201, linear in the radius", "markers_per_cell": "4x4",
+                       "per_body": "porosity U(0.05, 0.3), 26Al/27Al U(1e-5, 5e-5), "
+                                   "rock viscosity log-uniform 1e18-1e21 Pa s",
+                       "execution": "one host thread and stream per body; solver kernels "
+                                    "of all bodies on one shared stream",
+                       "precision": "fp64"}}
+
+
 def run_ours(args):
     rank, world, local = dist_setup(args.gpus)
     import torch
@@ -354,6 +400,7 @@ def run_ours(args):
     e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
     sim2.close()
     adj = None if args.no_adjoint else measure_adjoint(pkg, world)
+    ens = None if args.no_ensemble else measure_ensemble(pkg, world, rank, 16, 5, 2, 16)
     e2e = {"value": world * ne2e / (e2e_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
            "steps": ne2e}
@@ -421,7 +468,27 @@ def run_ours(args):
                                            for k, v in fstats.items()}}),
                 "roofline": roof, "roofline_solve": roof_solve, "phases": per,
                 "cpu_baseline": cpu, "clocks": ck, "e2e": e2e, "gpu_launches": launches,
-                "adjoint": adj}
+                "adjoint": adj, "ensemble": ens}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def run_ensemble(args):
+    """bench.py --workload ensemble: the ensemble line alone (default 256
+    bodies, 20 timed timesteps each after 3 untimed ones, 32 bodies at a
+    time)."""
+    rank, world, local = dist_setup(args.gpus)
+    pkg = load_pkg()
+    clocks = Clocks(local) if rank == 0 else None
+    line = measure_ensemble(pkg, world, rank, args.bodies, args.steps or 20, args.warmup,
+                            args.wave)
+    ck = clocks.stop() if clocks else None
+    if rank == 0:
+        line.update({"n_gpus": world, "higher_is_better": True, "scaling": "weak",
+                     "vs_baseline": None, "dtype": "f64", "data": "synthetic", "clocks": ck})
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -432,18 +499,34 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 50; ensemble workload: 20 per body)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint gradients/s measurement")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the 16-body ensemble measurement")
+    ap.add_argument("--bodies", type=int, default=256,
+                    help="ensemble workload: number of planetesimals")
+    ap.add_argument("--wave", type=int, default=32,
+                    help="ensemble workload: bodies resident at a time")
     ap.add_argument("--workload", default=WORKLOAD,
-                    choices=["planetesimal_41", "planetesimal_141", "planetesimal_401"])
+                    choices=["planetesimal_41", "planetesimal_141", "planetesimal_401",
+                             "ensemble"])
     ap.add_argument("--direct-solver", default="multifrontal", choices=["multifrontal", "band"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 multifrontal factors inside FP64 refinement")
     args = ap.parse_args()
+    if args.impl == "reference" and args.workload == "ensemble":
+        print(json.dumps({"impl": "reference", "unavailable": "the ensemble workload is "
+                          "timed on the GPU only; the CPU oracle takes ~10 s per 141x141 "
+                          "timestep, so its arm runs the single-body workloads"}))
+        return 0
+    if args.workload == "ensemble":
+        return run_ensemble(args)
+    args.steps = args.steps or 50
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -5,6 +5,8 @@
 // is enqueued on the state's stream; the host waits only where the
 // reference makes a decision (plastic and thermochemical convergence, the
 // dt updates, the new marker count).
+#include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -56,6 +58,33 @@ void timer_collect(erebus_state *s) {
         s->ev_pool.push_back(p.second.second);
     }
     s->ev_pending.clear();
+}
+
+// One stream per device for the cooperative launches of states that share it.
+static std::mutex g_coop_mutex;
+static cudaStream_t g_coop_stream[64];
+
+int coop_launch(erebus_state *s, const void *fn, int blocks, int threads, void **args,
+                size_t smem, const char *what) {
+    if (!s->shared_coop)
+        return check_cuda(s, cudaLaunchCooperativeKernel(fn, blocks, threads, args, smem,
+                                                         s->stream), what);
+    std::lock_guard<std::mutex> lock(g_coop_mutex);
+    if (s->device < 0 || s->device >= 64) return EREBUS_EINVAL;
+    cudaStream_t &cs = g_coop_stream[s->device];
+    if (!cs && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+        cs = nullptr;
+        return check_cuda(s, cudaErrorUnknown, "shared solver stream");
+    }
+    // the four calls run under the lock, so launches of different states
+    // follow one another on the shared stream without interleaving
+    int rc = check_cuda(s, cudaEventRecord(s->ev_to_coop, s->stream), what);
+    if (!rc) rc = check_cuda(s, cudaStreamWaitEvent(cs, s->ev_to_coop, 0), what);
+    if (!rc) rc = check_cuda(s, cudaLaunchCooperativeKernel(fn, blocks, threads, args, smem, cs),
+                             what);
+    if (!rc) rc = check_cuda(s, cudaEventRecord(s->ev_from_coop, cs), what);
+    if (!rc) rc = check_cuda(s, cudaStreamWaitEvent(s->stream, s->ev_from_coop, 0), what);
+    return rc;
 }
 }  // namespace erebus
 
@@ -228,8 +257,24 @@ int erebus_destroy(erebus_state *s) {
     if (s->snap_dev) cudaFree(s->snap_dev);
     if (s->snap_tm) cudaFreeHost(s->snap_tm);
     if (s->tm64) cudaFree(s->tm64);
+    if (s->ev_to_coop) cudaEventDestroy(s->ev_to_coop);
+    if (s->ev_from_coop) cudaEventDestroy(s->ev_from_coop);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
+    return EREBUS_OK;
+}
+
+int erebus_share_solver_stream(erebus_state *s, int32_t on) {
+    if (!s) return EREBUS_EINVAL;
+    cudaSetDevice(s->device);
+    if (on && !s->ev_to_coop) {
+        if (cudaEventCreateWithFlags(&s->ev_to_coop, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->ev_from_coop, cudaEventDisableTiming) != cudaSuccess) {
+            s->last_error = "share_solver_stream: event creation failed";
+            return EREBUS_ECUDA;
+        }
+    }
+    s->shared_coop = on != 0;
     return EREBUS_OK;
 }
 
@@ -491,6 +536,8 @@ int erebus_snapshot_begin(erebus_state *s, const ErebusGridHost *gh,
         if (s->snap_dev) cudaFree(s->snap_dev);
         if (s->snap_tm) cudaFreeHost(s->snap_tm);
     if (s->tm64) cudaFree(s->tm64);
+    if (s->ev_to_coop) cudaEventDestroy(s->ev_to_coop);
+    if (s->ev_from_coop) cudaEventDestroy(s->ev_from_coop);
         s->snap_dev = nullptr;
         s->snap_tm = nullptr;
         s->snap_cap = 0;

@@ -627,9 +627,7 @@ int band_factor(erebus_state *s, BandSystem &sys) {
     int *err = sys.err;
     void *args[] = {&B, &bar, &err};
     cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
-    int rc = check_cuda(s, cudaLaunchCooperativeKernel((const void *)k_band_factor, blocks,
-                                                       LU_THREADS, args, smem, s->stream),
-                        "band_factor launch");
+    int rc = coop_launch(s, (const void *)k_band_factor, blocks, LU_THREADS, args, smem, "band_factor launch");
     s->launches++;
     if (rc) return rc;
     sys.factored = true;

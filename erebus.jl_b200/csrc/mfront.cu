@@ -862,9 +862,7 @@ static int mf_factor_t(erebus_state *s, BandSystem &sys) {
     int *err = sys.err;
     void *args[] = {&V, &bar, &err};
     cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
-    rc = check_cuda(s, cudaLaunchCooperativeKernel(fn, blocks, LU_THREADS, args, smem,
-                                                   s->stream),
-                    "mf_factor launch");
+    rc = coop_launch(s, fn, blocks, LU_THREADS, args, smem, "mf_factor launch");
     s->launches++;
     return rc;
 }
@@ -922,9 +920,7 @@ int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
     int *err = sys.err;
     void *args[] = {&V, &w, &bar, &err};
     cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
-    int rc = check_cuda(s, cudaLaunchCooperativeKernel(fn, blocks, LU_THREADS, args, smem,
-                                                       s->stream),
-                        "mf_solve launch");
+    int rc = coop_launch(s, fn, blocks, LU_THREADS, args, smem, "mf_solve launch");
     s->launches++;
     return rc;
 }

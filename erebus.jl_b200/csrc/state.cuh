@@ -131,6 +131,10 @@ struct erebus_state {
     double snap_dt = 0.0, snap_timesum = 0.0;
     int64_t *snap_tm_dst = nullptr;
     int64_t *tm64 = nullptr;                   // int64 marker types (erebus_step_host)
+    // erebus_share_solver_stream: cooperative launches go to a per-device
+    // stream shared by all states that opted in
+    bool shared_coop = false;
+    cudaEvent_t ev_to_coop = nullptr, ev_from_coop = nullptr;
     double *partials = nullptr;                // reduction partials
     // replenishment scratch (per marker-grid anchor)
     unsigned long long *a_mdis = nullptr;
@@ -186,4 +190,9 @@ int build_cell_sort(erebus_state *s);
 // P-node sums of w * vals[m] over the markers in marker order (the scatter of
 // marker_to_p_nodes!, E:1814-1863), and of the weights, without normalising.
 int scatter_p_values(erebus_state *s, const double *vals, double *sum, double *wt);
+// Launches a grid-synchronised (cooperative) kernel for state s: on s->stream,
+// or, when the state shares the solver stream, on the per-device stream that
+// all such states share, ordered after s->stream's work and before its next.
+int coop_launch(erebus_state *s, const void *fn, int blocks, int threads, void **args,
+                size_t smem, const char *what);
 }  // namespace erebus

@@ -30,7 +30,7 @@ EXPORTS = [
     "erebus_advect_rk4", "erebus_replenish", "erebus_step", "erebus_export_hydromech",
     "erebus_apply_hydromech", "erebus_kernel_launches", "erebus_factor_stats",
     "erebus_snapshot_begin", "erebus_snapshot_wait", "erebus_adjoint_heat",
-    "erebus_step_host",
+    "erebus_step_host", "erebus_share_solver_stream",
 ]
 
 
@@ -63,6 +63,7 @@ def load_library(path=LIB_PATH):
         "erebus_check_params": [ctypes.POINTER(ErebusParams)],
         "erebus_create": [ctypes.POINTER(ErebusParams), I64, PP],
         "erebus_grid_layout": [ctypes.POINTER(ErebusParams), pI64, pI64],
+        "erebus_share_solver_stream": [P, I32],
         "erebus_destroy": [P],
         "erebus_set_solver_options": [P, ctypes.POINTER(ErebusSolverOptions)],
         "erebus_factor_stats": [P, I32, ctypes.POINTER(ErebusFactorStats)],
@@ -195,6 +196,13 @@ class Simulation:
         b, self._snapshot = self._snapshot, None
         b.marknum, b.dt, b.timesum = n.value, dt.value, ts.value
         return b
+
+    def share_solver_stream(self, on=True):
+        """Queue this state's grid-synchronised solver kernels on the stream
+        shared by all states that opted in (erebus_share_solver_stream), for
+        states stepped concurrently from several threads."""
+        self._check("erebus_share_solver_stream",
+                    self.L.erebus_share_solver_stream(self.h, 1 if on else 0))
 
     def set_solver_options(self, **kw):
         o = ErebusSolverOptions()

@@ -243,6 +243,15 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity,
 int erebus_grid_layout(const ErebusParams *p, int64_t *offsets, int64_t *total_bytes);
 int erebus_destroy(erebus_state *s);
 int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o);
+/* For states advanced concurrently from several host threads (an ensemble of
+   planetesimals): with on != 0 the state's grid-synchronised solver kernels
+   (factorisations and triangular solves: cooperative launches whose CTAs
+   wait for one another) are queued on one stream per device shared by all
+   states that opted in, so that two of them are never in flight together;
+   the state's other kernels stay on its own stream and overlap with other
+   states' work.  on = 0 restores the default (the state's own stream).  No
+   reference counterpart. */
+int erebus_share_solver_stream(erebus_state *s, int32_t on);
 /* Sizes and work of the direct solver of `system` (EREBUS_SYSTEM_*). */
 int erebus_factor_stats(erebus_state *s, int32_t system, ErebusFactorStats *out);
 /* Last CUDA/solver error text for a state (NUL-terminated, owned by state). */
