@@ -740,8 +740,8 @@ static int mf_grid(erebus_state *s) {
 // level's fronts each): the factor runs a front per CTA when that front's
 // tile operations are few, the solve when its tile sweeps are short.  The
 // thresholds come from timing each phase of the 141x141 systems on a B200.
-constexpr int kLocalFactorOps = 20;   // tile operations per CTA
-constexpr int kLocalSolveTiles = 48;  // tiles streamed per CTA and sweep
+constexpr int kLocalFactorOps = 8;    // tile operations per CTA
+constexpr int kLocalSolveTiles = 24;  // tiles streamed per CTA and sweep
 static std::vector<int> mf_level_modes(const MfPlan &P, int G) {
     std::vector<int> mode;
     for (size_t p = 0; p + 1 < P.level_begin.size(); p++) {
