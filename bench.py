@@ -448,7 +448,9 @@ def run_ours(args):
         cpu = None
         if not args.no_cpu_baseline and args.workload == WORKLOAD:
             cpu = cpu_baseline(pkg, load_oracle(), args.workload)
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        metric = METRIC if fp32 == 0 else \
+            "MIC timesteps/sec (mixed-precision GPU path: FP32 factors, FP64 refinement)"
+        line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
