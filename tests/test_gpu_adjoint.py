@@ -108,3 +108,22 @@ def test_autograd_function(pkg, built_lib):
     # a perturbed porosity reaches the device through forward()
     J2 = HeatObjective.apply(phim.detach() * 1.01, ratio.detach(), st, 3, 2)
     assert J2.item() != J0
+
+
+def test_device_adjoint_at_benchmark_size(pkg, oracle, built_lib):
+    """The bench's adjoint workload (141x141, 4x4 markers per cell, porosity
+    U(0.05, 0.25)) over two timesteps: device gradients equal the CPU
+    restatement's."""
+    import adjoint as AD
+    from erebus_b200.adjoint import at_rest
+    sg = at_rest(pkg.make_state("planetesimal_141_adjoint"))
+    so = at_rest(pkg.make_state("planetesimal_141_adjoint"))
+    sim = pkg.Simulation(sg)
+    J, dphi, dratio, stats = sim.adjoint_heat(2, checkpoint_every=1)
+    sim.close()
+    o, tape, W = AD.forward(so, 2)
+    phib, rbar = AD.adjoint(o, so, tape, W)
+    assert stats.markers == so.marknum == 313600
+    assert abs(J - AD.objective(so)) <= 1e-11 * abs(J)
+    np.testing.assert_allclose(dphi, phib, rtol=1e-7, atol=1e-9 * np.abs(phib).max())
+    assert abs(dratio - rbar) <= 1e-8 * abs(rbar)
