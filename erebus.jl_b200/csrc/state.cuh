@@ -47,6 +47,8 @@ struct DevScalars {
     double maxabs[8];          // reduction slots (bits of |x| as uint64)
     double sum_ddd;            // plastic yielding error sum of squares
     double norms[2];           // residual / right-hand side sums of squares
+    double norms0[2];          // the same at the start of a solve (first correction made
+                               // before they are read)
     int    ynpl;
     int    repl_count;         // markers to add in replenishment
     int    err;                // device-side error flag
@@ -88,6 +90,7 @@ struct BandSystem {
     int *err = nullptr;            // device error flag of the LU kernels
     bool factored = false;
     bool have_x = false;           // x holds a converged solution
+    bool warm_ok = false;          // the last solve's starting point already met the target
     int factorizations = 0;        // number of factorisations so far
     int fp64_refactorizations = 0; // FP64 factorisations after stalled FP32 refinement
     int ph_factor = -1, ph_solve = -1;   // timer phases of this system
