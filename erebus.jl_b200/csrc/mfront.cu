@@ -47,6 +47,7 @@ struct MfView {
     const int *lvl;     // level ranges (nlev + 1)
     const int *lvl_kt;  // max Kt per level
     const int *lvl_mode;  // per level: MF_FACTOR_LOCAL, MF_SOLVE_LOCAL bits
+    int *flags;         // per 64-row block of the front vectors: the solve epoch it is final in
     int nlev;
     const long long *target;   // ELL entry -> storage offset
     const int *expect;         // ELL column pattern the targets were built from
@@ -62,6 +63,8 @@ struct MfDevice {
     double *vec = nullptr;
     int *vars = nullptr, *eamap = nullptr, *lvl = nullptr, *lvl_kt = nullptr;
     int *lvl_mode = nullptr;
+    int *flags = nullptr;   // row-block flags of the cooperative solve levels
+    int epoch = 0;          // solves launched so far
     long long *target = nullptr;
     int *expect = nullptr;
     int nlev = 0;
@@ -608,10 +611,140 @@ __device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, doubl
         err);
 }
 
+// ---- cooperative levels: one task per 64-row block of a front --------------
+// Row block I of front f is final in solve `epoch` once its flag holds
+// 2 epoch (forward) or 2 epoch + 1 (backward); epochs grow, so older marks
+// are smaller.  Writers: every thread fences its own stores, then thread 0
+// raises the flag; readers: thread 0 waits (bounded, 2 s; on timeout *err = 3)
+// and the block reads through L2.
+__device__ __forceinline__ int *mf_flag(const MfView &V, const MfFront &f, int I) {
+    return V.flags + f.vec_off / 64 + I;
+}
+__device__ __forceinline__ void mf_wait_flag(const int *flag, int want, int *err) {
+    if (threadIdx.x == 0) {
+        unsigned long long t0 = 0;
+        for (int spin = 0;; spin++) {
+            if (*(volatile const int *)flag >= want) break;
+            if (spin == 0) {
+                t0 = globaltimer();
+            } else if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
+                atomicExch(err, 3);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ void mf_raise_flag(int *flag, int val) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicExch(flag, val);
+}
+
+// Element a of front f's vector before elimination: the right-hand side of
+// an eliminated unknown plus the children's update entries (child 0, then
+// child 1).
+__device__ __forceinline__ double mf_gather_elem(const MfView &V, const MfFront &f,
+                                                 const double *w, int a, bool h0,
+                                                 const MfFront &C0, bool h1,
+                                                 const MfFront &C1) {
+    const int *var = V.vars + f.var_off, *map = V.eamap + f.map_off;
+    int g = var[a];
+    double s = (a < f.Kp && g >= 0) ? __ldcg(&w[g]) : 0.0;
+    if (h0) {
+        int i = map[2 * a];
+        if (i >= 0) s += __ldcg(&V.vec[C0.vec_off + C0.Kp + i]);
+    }
+    if (h1) {
+        int i = map[2 * a + 1];
+        if (i >= 0) s += __ldcg(&V.vec[C1.vec_off + C1.Kp + i]);
+    }
+    return s;
+}
+
+// Forward, row block I: v_I = gather_I - sum_{K < min(I, Kt)} L_IK y_K, the
+// y_K taken as their rows finish; pivot rows then publish.
+template <class T>
+__device__ void mf_fwd_row(const MfView &V, const MfFront &f, const double *w, int I, int epoch,
+                           MfSolveSmem &S, uint32_t *uses, int *err) {
+    double *v = V.vec + f.vec_off;
+    const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
+    MfFront C0, C1;
+    if (h0) C0 = V.fr[f.c0];
+    if (h1) C1 = V.fr[f.c1];
+    double gath = 0.0;
+    if (threadIdx.x < 64) gath = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
+    const int nK = I < f.Kt ? I : f.Kt;
+    double acc = 0.0;
+    mf_stream(
+        S, uses, nK, [&](int K) { return (const T *)ftile<T>(V, f, I, K); },
+        [&](int K, const T *Tt) {
+            mf_wait_flag(mf_flag(V, f, K), 2 * epoch, err);
+            if (threadIdx.x < 64) S.x[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
+            __syncthreads();
+            acc += mf_quarter(Tt, S.x);
+        },
+        err);
+    double t = mf_reduce_rows(S, acc);
+    if (threadIdx.x < 64) __stcg(&v[I * 64 + threadIdx.x], gath - t);
+    if (I < f.Kt) mf_raise_flag(mf_flag(V, f, I), 2 * epoch);
+    __syncthreads();
+}
+
+// Backward, row block K of the pivot part:
+// x_K = D_K^{-1} (v_K - sum_{J >= Kt} U_KJ x_J - sum_{K < J < Kt} U_KJ x_J),
+// the ring solution from w, the pivot ones taken as their rows finish.
+template <class T>
+__device__ void mf_bwd_row(const MfView &V, const MfFront &f, double *w, int K, int epoch,
+                           MfSolveSmem &S, uint32_t *uses, int *err) {
+    double *v = V.vec + f.vec_off;
+    const int *var = V.vars + f.var_off;
+    const int nr = f.Mt - f.Kt, np = f.Kt - 1 - K;
+    double acc = 0.0;
+    mf_stream(
+        S, uses, nr + np + 1,
+        [&](int i) {
+            const int J = i < nr ? f.Kt + i : i < nr + np ? f.Kt - 1 - (i - nr) : K;
+            return (const T *)ftile<T>(V, f, K, J);
+        },
+        [&](int i, const T *Tt) {
+            if (i < nr) {
+                const int J = f.Kt + i;
+                if (threadIdx.x < 64) {
+                    int g = var[J * 64 + threadIdx.x];
+                    S.x[threadIdx.x] = g >= 0 ? __ldcg(&w[g]) : 0.0;
+                }
+                __syncthreads();
+                acc += mf_quarter(Tt, S.x);
+            } else if (i < nr + np) {
+                const int J = f.Kt - 1 - (i - nr);
+                mf_wait_flag(mf_flag(V, f, J), 2 * epoch + 1, err);
+                if (threadIdx.x < 64) S.x[threadIdx.x] = __ldcg(&v[J * 64 + threadIdx.x]);
+                __syncthreads();
+                acc += mf_quarter(Tt, S.x);
+            } else {   // the diagonal tile holds D_K^{-1}
+                double t = mf_reduce_rows(S, acc);
+                if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]) - t;
+                __syncthreads();
+                double x = mf_reduce_rows(S, mf_quarter(Tt, S.y));
+                if (threadIdx.x < 64) {
+                    const int a = K * 64 + threadIdx.x;
+                    __stcg(&v[a], x);
+                    if (a < f.k) __stcg(&w[var[a]], x);
+                }
+            }
+        },
+        err);
+    mf_raise_flag(mf_flag(V, f, K), 2 * epoch + 1);
+    __syncthreads();
+}
+
 // Solves L U x = w in place (w: n values; rows >= n untouched).
 template <class T>
 __global__ void __launch_bounds__(LU_THREADS, 2)
-k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
+k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
     extern __shared__ __align__(128) double smem_raw[];
     MfSolveSmem &S = *reinterpret_cast<MfSolveSmem *>(smem_raw);
     const int G = gridDim.x;
@@ -630,23 +763,18 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
         const bool local = V.lvl_mode[p] & MF_SOLVE_LOCAL;
         if (!local) mf_load_km(V, fb, fe, S.km);
-        for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
-            const MfFront f = V.fr[fi];
-            double *v = V.vec + f.vec_off;
-            mf_gather_fwd(V, f, w, v);
-            mf_fwd_front<T>(V, f, v, local ? f.Mt : f.Kt, S, uses, err);
-        }
-        if (!local) {
-            grid_barrier(bar, err);
-            // update rows: v_I -= sum_{K < Kt} L_IK y_K
+        if (local) {
+            for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
+                const MfFront f = V.fr[fi];
+                double *v = V.vec + f.vec_off;
+                mf_gather_fwd(V, f, w, v);
+                mf_fwd_front<T>(V, f, v, f.Mt, S, uses, err);
+            }
+        } else {
+            // one task per row block, in increasing order within each front
             mf_for_tasks(
-                V, fb, fe, S.km, [](int Kt, int Mt) { return Mt - Kt; },
-                [&](const MfFront &f, int u) {
-                    double *v = V.vec + f.vec_off;
-                    mf_row_gemv<T>(
-                        V, f, v, f.Kt + u, 0, f.Kt,
-                        [&](int K, int c) { return __ldcg(&v[K * 64 + c]); }, S, uses, err);
-                });
+                V, fb, fe, S.km, [](int, int Mt) { return Mt; },
+                [&](const MfFront &f, int I) { mf_fwd_row<T>(V, f, w, I, epoch, S, uses, err); });
         }
         grid_barrier(bar, err);
     }
@@ -662,23 +790,21 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err) {
                 return g >= 0 ? __ldcg(&w[g]) : 0.0;
             };
         };
-        if (!local) {
-            // eliminated rows: v_K -= sum_{J >= Kt} U_KJ x_J
-            mf_for_tasks(
-                V, fb, fe, S.km, [](int Kt, int Mt) { return Mt > Kt ? Kt : 0; },
-                [&](const MfFront &f, int u) {
-                    mf_row_gemv<T>(V, f, V.vec + f.vec_off, u, f.Kt, f.Mt, ring_x(f), S, uses,
-                                   err);
-                });
-            grid_barrier(bar, err);
-        }
-        for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
-            const MfFront f = V.fr[fi];
-            double *v = V.vec + f.vec_off;
-            if (local)
+        if (local) {
+            for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
+                const MfFront f = V.fr[fi];
+                double *v = V.vec + f.vec_off;
                 for (int K = 0; K < f.Kt && f.Mt > f.Kt; K++)
                     mf_row_gemv<T>(V, f, v, K, f.Kt, f.Mt, ring_x(f), S, uses, err);
-            mf_bwd_front<T>(V, f, v, w, S, uses, err);
+                mf_bwd_front<T>(V, f, v, w, S, uses, err);
+            }
+        } else {
+            // one task per pivot row block, the last first
+            mf_for_tasks(
+                V, fb, fe, S.km, [](int Kt, int) { return Kt; },
+                [&](const MfFront &f, int u) {
+                    mf_bwd_row<T>(V, f, w, f.Kt - 1 - u, epoch, S, uses, err);
+                });
         }
         grid_barrier(bar, err);
     }
@@ -697,6 +823,7 @@ static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
     V.lvl = D.lvl;
     V.lvl_kt = D.lvl_kt;
     V.lvl_mode = D.lvl_mode;
+    V.flags = D.flags;
     V.nlev = D.nlev;
     V.target = D.target;
     V.expect = D.expect;
@@ -711,7 +838,7 @@ void mf_release(BandSystem &sys) {
     MfDevice *D = sys.mf;
     if (!D) return;
     void *ps[] = {D->fr, D->F64, D->F32, D->vec, D->vars, D->eamap, D->lvl, D->lvl_kt,
-                  D->lvl_mode, D->target, D->expect};
+                  D->lvl_mode, D->flags, D->target, D->expect};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete D;
@@ -815,6 +942,9 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
     if (e == cudaSuccess) e = upload(&D->target, target, s->stream);
     if (e == cudaSuccess) e = upload(&D->expect, expect, s->stream);
     if (e == cudaSuccess) e = cudaMalloc(&D->vec, P.vec * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&D->flags, (P.vec / MF_TILE + 1) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(D->flags, 0, (P.vec / MF_TILE + 1) * sizeof(int),
+                                              s->stream);
     if (e != cudaSuccess) {
         s->last_error = std::string("multifrontal allocation: ") + cudaGetErrorString(e);
         return EREBUS_ENOMEM;
@@ -918,7 +1048,8 @@ int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
     }
     unsigned int *bar = sys.bar;
     int *err = sys.err;
-    void *args[] = {&V, &w, &bar, &err};
+    int epoch = ++D.epoch;
+    void *args[] = {&V, &w, &bar, &err, &epoch};
     cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
     int rc = coop_launch(s, fn, blocks, LU_THREADS, args, smem, "mf_solve launch");
     s->launches++;
