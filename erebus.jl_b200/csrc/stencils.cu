@@ -20,6 +20,18 @@ __device__ __forceinline__ void amax(double *slot, double v) {
     atomicMax(reinterpret_cast<unsigned long long *>(slot),
               (unsigned long long)__double_as_longlong(fabs(v)));
 }
+// The same maximum of |v| (as bits, so NaN wins as before), reduced over the
+// warp first: one atomic per warp.  Every lane of the warp calls it; lanes
+// without a value pass active = false.
+__device__ __forceinline__ void amax_warp(double *slot, double v, bool active) {
+    unsigned long long b = active ? (unsigned long long)__double_as_longlong(fabs(v)) : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long c = __shfl_xor_sync(0xffffffffu, b, o);
+        b = c > b ? c : b;
+    }
+    if ((threadIdx.x & 31) == 0 && b) atomicMax(reinterpret_cast<unsigned long long *>(slot), b);
+}
 
 #define NODE_P(g, t)                                  \
     int t = blockIdx.x * blockDim.x + threadIdx.x;    \
@@ -65,14 +77,18 @@ __global__ void k_hydro_post(ErebusParams p, Geo g, GridPtrs G, const double *S)
 
 // compute_Aphi! (E:3675-3689) on [2:Ny, 2:Nx]; max |APHI| -> maxabs[X_APHI]
 __global__ void k_aphi(Geo g, GridPtrs G, DevScalars *sc) {
-    NODE_P(g, t);
-    if (i < 2 || i > g.Ny || j < 2 || j > g.Nx) return;
-    double dt = sc->dt;
-    double pr = G.pr[t], pf = G.pf[t], ph = G.PHI[t];
-    double v = ((pr - pf) / G.ETAPHI[t] + ((pr - G.pr0[t]) - (pf - G.pf0[t])) / dt * G.BETAPHI[t]) /
-               (1 - ph) / ph;
-    G.APHI[t] = v;
-    amax(&sc->maxabs[X_APHI], v);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t % g.Ny1 + 1, j = t / g.Ny1 + 1;
+    const bool in = t < g.Ny1 * g.Nx1 && i >= 2 && i <= g.Ny && j >= 2 && j <= g.Nx;
+    double v = 0.0;
+    if (in) {
+        double dt = sc->dt;
+        double pr = G.pr[t], pf = G.pf[t], ph = G.PHI[t];
+        v = ((pr - pf) / G.ETAPHI[t] + ((pr - G.pr0[t]) - (pf - G.pf0[t])) / dt * G.BETAPHI[t]) /
+            (1 - ph) / ph;
+        G.APHI[t] = v;
+    }
+    amax_warp(&sc->maxabs[X_APHI], v, in);
 }
 
 // compute_fluid_velocities! (E:3716-3757), first half: the values before
@@ -105,15 +121,21 @@ __global__ void k_fluid_pre(ErebusParams p, Geo g, GridPtrs G, double *tx, doubl
 // compute_displacement_timestep (E:3786-3789)
 __global__ void k_fluid_fin(Geo g, GridPtrs G, const double *tx, const double *ty,
                             DevScalars *sc) {
-    NODE_P(g, t);
-    (void)i; (void)j;
-    double a = tx[t] + G.vx[t], b = ty[t] + G.vy[t];
-    G.vxf[t] = a;
-    G.vyf[t] = b;
-    amax(&sc->maxabs[X_VX], G.vx[t]);
-    amax(&sc->maxabs[X_VY], G.vy[t]);
-    amax(&sc->maxabs[X_VXF], a);
-    amax(&sc->maxabs[X_VYF], b);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = t < g.Ny1 * g.Nx1;
+    double vx = 0.0, vy = 0.0, a = 0.0, b = 0.0;
+    if (in) {
+        vx = G.vx[t];
+        vy = G.vy[t];
+        a = tx[t] + vx;
+        b = ty[t] + vy;
+        G.vxf[t] = a;
+        G.vyf[t] = b;
+    }
+    amax_warp(&sc->maxabs[X_VX], vx, in);
+    amax_warp(&sc->maxabs[X_VY], vy, in);
+    amax_warp(&sc->maxabs[X_VXF], a, in);
+    amax_warp(&sc->maxabs[X_VYF], b, in);
 }
 
 // compute_displacement_timestep (E:3777-3803)
@@ -301,15 +323,20 @@ __global__ void k_adiabatic_heating(Geo g, GridPtrs G) {
 // tk2 from the solution, DT = tk2 - tk1 (E:6926-6927) and the maxima of
 // E:6929, E:4218-4219
 __global__ void k_thermal_post(Geo g, GridPtrs G, const double *S, DevScalars *sc) {
-    NODE_P(g, t);
-    (void)i; (void)j;
-    double tk2 = S[t];
-    G.tk2[t] = tk2;
-    double d = tk2 - G.tk1[t];
-    G.DT[t] = d;
-    amax(&sc->maxabs[X_DT], d);
-    amax(&sc->maxabs[X_PFERR], G.pf[t] - G.pf0[t]);
-    amax(&sc->maxabs[X_DMP], G.DMP[t]);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = t < g.Ny1 * g.Nx1;
+    double d = 0.0, e = 0.0, m = 0.0;
+    if (in) {
+        double tk2 = S[t];
+        G.tk2[t] = tk2;
+        d = tk2 - G.tk1[t];
+        G.DT[t] = d;
+        e = G.pf[t] - G.pf0[t];
+        m = G.DMP[t];
+    }
+    amax_warp(&sc->maxabs[X_DT], d, in);
+    amax_warp(&sc->maxabs[X_PFERR], e, in);
+    amax_warp(&sc->maxabs[X_DMP], m, in);
 }
 
 // compute_velocities! (E:4878-4928): interior, then rows, then columns
