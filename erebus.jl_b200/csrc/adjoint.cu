@@ -186,7 +186,9 @@ __global__ void k_adj_assemble(Geo g, const double *rhocp, const double *KX,
         B.ell_vals[r * B.ell + k] = v;
         diff |= __double_as_longlong(prev[r * B.ell + k]) != __double_as_longlong(v);
     }
-    if (diff) atomicOr(changed, 1);
+    // one atomic per warp (every changed row of a refactored matrix sets it)
+    const unsigned am = __activemask(), any = __ballot_sync(am, diff);
+    if (any && (threadIdx.x & 31) == __ffs(am) - 1) atomicOr(changed, 1);
 }
 
 struct AdjNodeIn {

@@ -304,7 +304,9 @@ __global__ void k_assemble_ell(int kind, ErebusParams p, Geo g, GridPtrs G,
             diff |= __double_as_longlong(prev[row * B.ell + k]) != __double_as_longlong(v);
         }
     }
-    if (diff) atomicOr(changed, 1);
+    // one atomic per warp (every changed row of a refactored matrix sets it)
+    const unsigned am = __activemask(), any = __ballot_sync(am, diff);
+    if (any && (threadIdx.x & 31) == __ffs(am) - 1) atomicOr(changed, 1);
 }
 
 // Scaled ELL rows -> block-banded tiles (zeroed beforehand); also keeps the
