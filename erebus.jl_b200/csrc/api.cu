@@ -331,6 +331,8 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
     }
     s->tm8 = (int8_t *)alloc(cap);
     if (!s->tm8) return fail(EREBUS_ENOMEM, "markers");
+    s->wcache = (double *)alloc(cap * 16 * sizeof(double));
+    if (!s->wcache) return fail(EREBUS_ENOMEM, "marker weights");
     {   // one slab in the layout of erebus_grid_layout
         int64_t off[G_COUNT], total = 0;
         erebus_grid_layout(p, off, &total);

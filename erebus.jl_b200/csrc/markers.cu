@@ -98,6 +98,26 @@ __global__ void k_sort_count(Geo g, const double *xm, const double *ym, int n,
     for (int gr = 0; gr < 4; gr++) atomicAdd(&S.count[gr][cell_of(g, gr, x, y)], 1);
 }
 
+// Bilinear weights of every marker on the four node sets (fix_weights,
+// E:1388), wc[(grid * cap + m) * 4 + k].  They hold while the markers do not
+// move (as the cell sort does), and the merges read them instead of
+// recomputing them at every node visit.
+__global__ void k_marker_weights(Geo g, const double *xm, const double *ym, int n, int64_t cap,
+                                 double *wc) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    double x = xm[m], y = ym[m];
+#pragma unroll
+    for (int gr = 0; gr < 4; gr++) {
+        int i, j;
+        double w[4];
+        grid_weights(g, gr, x, y, i, j, w);
+        double2 *d = reinterpret_cast<double2 *>(wc + ((size_t)gr * cap + m) * 4);
+        d[0] = make_double2(w[0], w[1]);
+        d[1] = make_double2(w[2], w[3]);
+    }
+}
+
 // Exclusive scan of count -> start (start[ncells] = total), one block per grid.
 __global__ void k_sort_scan(SortPtrs S) {
     int gr = blockIdx.x;
@@ -262,6 +282,8 @@ struct MergeArgs {
     const int8_t *flag;        // reaction: only flagged markers contribute
     const double *dM, *dH;
     double *sums[10];          // destination SUM arrays
+    const double *wc;          // the markers' weights on this grid (k_marker_weights), or
+                               // NULL: computed at each visit
 };
 
 template <int GRID, int MODE>
@@ -298,10 +320,15 @@ __global__ void k_merge(Geo g, MP M, MergeArgs a, GPtr G, int write_props) {
         if (best < 0) break;
         beg[best]++;
         if (MODE == MM_REACTION && !a.flag[bm]) continue;
-        int i, j;
-        double w[4];
-        grid_weights(g, GRID, xm[bm], ym[bm], i, j, w);
-        double wk = best == 0 ? w[0] : best == 1 ? w[1] : best == 2 ? w[2] : w[3];
+        double wk;
+        if (a.wc) {
+            wk = a.wc[(size_t)bm * 4 + best];
+        } else {
+            int i, j;
+            double w[4];
+            grid_weights(g, GRID, xm[bm], ym[bm], i, j, w);
+            wk = best == 0 ? w[0] : best == 1 ? w[1] : best == 2 ? w[2] : w[3];
+        }
         double v[F::N];
         F::load(M, a.dM, a.dH, bm, v);
 #pragma unroll
@@ -415,6 +442,8 @@ int build_cell_sort(erebus_state *s) {
     if (n > 0) {
         EREBUS_LAUNCH(s, k_sort_count, nblocks(n), kThreads, 0, s->g, s->m[M_xm],
                       s->m[M_ym], n, S);
+        EREBUS_LAUNCH(s, k_marker_weights, nblocks(n), kThreads, 0, s->g, s->m[M_xm],
+                      s->m[M_ym], n, s->capacity, s->wcache);
     }
     EREBUS_LAUNCH(s, k_sort_scan, 4, 1024, 0, S);
     if (n > 0) {
@@ -439,6 +468,7 @@ static MergeArgs merge_args(erebus_state *s, int gr, std::initializer_list<int> 
     MergeArgs a = {};
     a.start = s->sort[gr].start;
     a.idx = s->sort[gr].idx;
+    a.wc = s->wcache + (size_t)gr * s->capacity * 4;
     a.flag = s->r_flag;
     a.dM = s->r_dM;
     a.dH = s->r_dH;
@@ -455,6 +485,7 @@ int scatter_p_values(erebus_state *s, const double *vals, double *sum, double *w
     MergeArgs a = {};
     a.start = s->sort[GP].start;
     a.idx = s->sort[GP].idx;
+    a.wc = s->wcache + (size_t)GP * s->capacity * 4;
     a.dM = vals;
     a.sums[0] = sum;
     a.sums[1] = wt;

@@ -122,6 +122,7 @@ struct erebus_state {
     double *r_dM = nullptr, *r_dH = nullptr;   // per-marker reaction outputs
     int8_t *r_flag = nullptr;
     double *tmp_node = nullptr;                // node-sized scratch
+    double *wcache = nullptr;                  // markers' weights on the 4 node sets
     double *norm_part = nullptr;               // partial sums of the residual norms
     // asynchronous snapshot (erebus_snapshot_begin / _wait)
     cudaStream_t copy_stream = nullptr;
