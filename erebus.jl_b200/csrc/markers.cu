@@ -286,14 +286,10 @@ struct MergeArgs {
                                // NULL: computed at each visit
 };
 
-template <int GRID, int MODE>
-__global__ void k_merge(Geo g, MP M, MergeArgs a, GPtr G, int write_props) {
-    using F = MergeFields<GRID, MODE>;
-    GridSpec s = grid_spec(g, GRID);
-    int node = blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= s.rows * s.cols) return;
-    int I = node % s.rows + 1, J = node / s.rows + 1;
-    int beg[4], end[4];
+// Bucket bounds of node (I,J): the cells (I,J), (I-1,J), (I,J-1), (I-1,J-1),
+// with weights w0..w3 (E:1517).
+__device__ __forceinline__ void node_buckets(const GridSpec &s, const MergeArgs &a, int I,
+                                             int J, int beg[4], int end[4]) {
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         int ci = I - (k & 1), cj = J - (k >> 1);
@@ -305,10 +301,27 @@ __global__ void k_merge(Geo g, MP M, MergeArgs a, GPtr G, int write_props) {
             beg[k] = end[k] = 0;
         }
     }
-    double acc[F::N];
+}
+
+// Weight of marker m on corner k of its cell.
+template <int GRID>
+__device__ __forceinline__ double merge_weight(const Geo &g, const MP &M, const MergeArgs &a,
+                                               int m, int k) {
+    if (a.wc) return a.wc[(size_t)m * 4 + k];
+    int i, j;
+    double w[4];
+    grid_weights(g, GRID, M.f[M_xm][m], M.f[M_ym][m], i, j, w);
+    return k == 0 ? w[0] : k == 1 ? w[1] : k == 2 ? w[2] : w[3];
+}
+
+// One thread walks the four buckets in marker order and sums every field.
+template <int GRID, int MODE>
+__device__ __forceinline__ void merge_serial(const Geo &g, const MP &M, const MergeArgs &a,
+                                             int beg[4], const int end[4],
+                                             double (&acc)[MergeFields<GRID, MODE>::N]) {
+    using F = MergeFields<GRID, MODE>;
 #pragma unroll
     for (int f = 0; f < F::N; f++) acc[f] = 0.0;
-    const double *xm = M.f[M_xm], *ym = M.f[M_ym];
     while (true) {
         int best = -1, bm = INT_MAX;
 #pragma unroll
@@ -320,20 +333,21 @@ __global__ void k_merge(Geo g, MP M, MergeArgs a, GPtr G, int write_props) {
         if (best < 0) break;
         beg[best]++;
         if (MODE == MM_REACTION && !a.flag[bm]) continue;
-        double wk;
-        if (a.wc) {
-            wk = a.wc[(size_t)bm * 4 + best];
-        } else {
-            int i, j;
-            double w[4];
-            grid_weights(g, GRID, xm[bm], ym[bm], i, j, w);
-            wk = best == 0 ? w[0] : best == 1 ? w[1] : best == 2 ? w[2] : w[3];
-        }
+        double wk = merge_weight<GRID>(g, M, a, bm, best);
         double v[F::N];
         F::load(M, a.dM, a.dH, bm, v);
 #pragma unroll
         for (int f = 0; f < F::N; f++) acc[f] = acc[f] + v[f] * wk;
     }
+}
+
+// The SUM arrays of a node and the node properties computed from them.
+template <int GRID, int MODE>
+__device__ __forceinline__ void merge_finish(const Geo &g, const MergeArgs &a, const GPtr &G,
+                                             int node, int I, int J,
+                                             const double (&acc)[MergeFields<GRID, MODE>::N],
+                                             int write_props) {
+    using F = MergeFields<GRID, MODE>;
 #pragma unroll
     for (int f = 0; f < F::N; f++) a.sums[f][node] = acc[f];
     if (!write_props) return;
@@ -403,6 +417,159 @@ __global__ void k_merge(Geo g, MP M, MergeArgs a, GPtr G, int write_props) {
     }
 }
 
+
+// One thread per node.
+template <int GRID, int MODE>
+__global__ void k_merge(Geo g, MP M, MergeArgs a, GPtr G, int write_props) {
+    using F = MergeFields<GRID, MODE>;
+    GridSpec s = grid_spec(g, GRID);
+    int node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= s.rows * s.cols) return;
+    int I = node % s.rows + 1, J = node / s.rows + 1;
+    int beg[4], end[4];
+    node_buckets(s, a, I, J, beg, end);
+    double acc[F::N];
+    merge_serial<GRID, MODE>(g, M, a, beg, end, acc);
+    merge_finish<GRID, MODE>(g, a, G, node, I, J, acc, write_props);
+}
+
+// One warp per node.  The lanes copy the node's four sorted buckets into
+// shared memory and place every marker at its rank in the merged marker
+// order (its position in its bucket plus, by binary search, the number of
+// smaller marker numbers in the other three).  Then, a window of positions
+// at a time, the lanes load the markers' values and weights in parallel and
+// store the products, and lane f adds field f's products in merged order.
+// The products and the order of the additions are those of the one-thread
+// walk, so the sums are the same bits.  Nodes with more than kMergeCap
+// markers take the one-thread walk on lane 0.
+constexpr int kMergeWarps = 4;      // nodes per block
+constexpr int kMergeCap = 256;      // markers of a node held in shared memory
+constexpr int kMergeWin = 64;       // merged positions per product window (two per lane)
+
+// Rank of v in the merged order: the number of smaller keys in the four
+// sorted buckets key[b[k], b[k] + n[k]) (in its own bucket, its position).
+// The four searches advance together; their trip counts depend only on the
+// bucket lengths, which all lanes of the warp share.
+__device__ __forceinline__ int merged_rank(const int *key, const int b[4], const int n[4],
+                                           int v) {
+    int lo[4], len[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) { lo[k] = b[k]; len[k] = n[k]; }
+    while (max(max(len[0], len[1]), max(len[2], len[3])) > 1) {
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (len[k] > 1) {
+                int h = len[k] >> 1;
+                lo[k] += key[lo[k] + h - 1] < v ? h : 0;
+                len[k] -= h;
+            }
+    }
+    int r = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) r += lo[k] - b[k] + (len[k] == 1 && key[lo[k]] < v ? 1 : 0);
+    return r;
+}
+
+template <int GRID, int MODE>
+__global__ void __launch_bounds__(kMergeWarps * 32)
+k_merge_warp(Geo g, MP M, MergeArgs a, GPtr G, int write_props) {
+    using F = MergeFields<GRID, MODE>;
+    constexpr int N = F::N;
+    __shared__ int s_key[kMergeWarps][kMergeCap];
+    __shared__ unsigned short s_ord[kMergeWarps][kMergeCap];
+    __shared__ double s_prod[kMergeWarps][N][kMergeWin + 1];
+    GridSpec s = grid_spec(g, GRID);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int node = blockIdx.x * kMergeWarps + w;
+    if (node >= s.rows * s.cols) return;        // uniform over the warp
+    const int I = node % s.rows + 1, J = node / s.rows + 1;
+    int beg[4], end[4];
+    node_buckets(s, a, I, J, beg, end);
+    const int o1 = end[0] - beg[0], o2 = o1 + end[1] - beg[1], o3 = o2 + end[2] - beg[2];
+    int L = o3 + end[3] - beg[3];
+    double acc[N];
+    if (L > kMergeCap) {
+        if (lane == 0) {
+            merge_serial<GRID, MODE>(g, M, a, beg, end, acc);
+            merge_finish<GRID, MODE>(g, a, G, node, I, J, acc, write_props);
+        }
+        return;
+    }
+    int *key = s_key[w];
+    unsigned short *ord = s_ord[w];
+    for (int e = lane; e < L; e += 32) {
+        int k = e < o1 ? 0 : e < o2 ? 1 : e < o3 ? 2 : 3;
+        int o = k == 0 ? 0 : k == 1 ? o1 : k == 2 ? o2 : o3;
+        key[e] = a.idx[beg[k] + e - o];
+    }
+    __syncwarp();
+    {
+        const int bb[4] = {0, o1, o2, o3}, nn[4] = {o1, o2 - o1, o3 - o2, L - o3};
+        for (int e = lane; e < L; e += 32) ord[merged_rank(key, bb, nn, key[e])] = e;
+    }
+    __syncwarp();
+    if (MODE == MM_REACTION) {
+        // keep the flagged markers, in merged order
+        int kept = 0;
+        for (int r0 = 0; r0 < L; r0 += 32) {
+            int r = r0 + lane;
+            unsigned short e = 0;
+            bool keep = false;
+            if (r < L) {
+                e = ord[r];
+                keep = a.flag[key[e]] != 0;
+            }
+            unsigned b = __ballot_sync(0xffffffffu, keep);
+            __syncwarp();
+            if (keep) ord[kept + __popc(b & ((1u << lane) - 1u))] = e;
+            kept += __popc(b);
+            __syncwarp();
+        }
+        L = kept;
+    }
+    double sum = 0.0;
+    double (*prod)[kMergeWin + 1] = s_prod[w];
+    for (int r0 = 0; r0 < L; r0 += kMergeWin) {
+        const int cnt = min(kMergeWin, L - r0);
+        // positions lane and lane + 32 of the window, loads issued together
+        double wk[2], v[2][N];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int t = lane + 32 * u;
+            if (t < cnt) {
+                int e = ord[r0 + t];
+                int k = e < o1 ? 0 : e < o2 ? 1 : e < o3 ? 2 : 3;
+                int m = key[e];
+                wk[u] = merge_weight<GRID>(g, M, a, m, k);
+                F::load(M, a.dM, a.dH, m, v[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+            if (lane + 32 * u < cnt) {
+#pragma unroll
+                for (int f = 0; f < N; f++) prod[f][lane + 32 * u] = v[u][f] * wk[u];
+            }
+        __syncwarp();
+        if (lane < N) {
+            const double *q = prod[lane];
+            int t = 0;
+            for (; t + 8 <= cnt; t += 8) {
+                double x[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) x[u] = q[t + u];
+#pragma unroll
+                for (int u = 0; u < 8; u++) sum = sum + x[u];
+            }
+            for (; t < cnt; t++) sum = sum + q[t];
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int f = 0; f < N; f++) acc[f] = __shfl_sync(0xffffffffu, sum, f);
+    if (lane == 0) merge_finish<GRID, MODE>(g, a, G, node, I, J, acc, write_props);
+}
+
 // apply_insulating_boundary_conditions! (E:2432-2449) on tk1, two passes
 __global__ void k_insulate_rows(Geo g, double *t) {
     int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
@@ -460,8 +627,9 @@ int build_cell_sort(erebus_state *s) {
 template <int GRID, int MODE>
 static void launch_merge(erebus_state *s, MergeArgs a, int write_props) {
     GridSpec sp = grid_spec(s->g, GRID);
-    EREBUS_LAUNCH(s, (k_merge<GRID, MODE>), nblocks((int64_t)sp.rows * sp.cols, 128), 128, 0,
-                  s->g, mptr(s), a, gptr(s), write_props);
+    EREBUS_LAUNCH(s, (k_merge_warp<GRID, MODE>),
+                  nblocks((int64_t)sp.rows * sp.cols, kMergeWarps), kMergeWarps * 32, 0, s->g,
+                  mptr(s), a, gptr(s), write_props);
 }
 
 static MergeArgs merge_args(erebus_state *s, int gr, std::initializer_list<int> sums) {
