@@ -650,6 +650,10 @@ static int band_solve_inplace(erebus_state *s, BandSystem &sys, double *w) {
     return check_cuda(s, cudaGetLastError(), "band_solve launch");
 }
 
+// Solves accepted at a system's measured residual floor before refinement is
+// run to the stall again.
+constexpr int kFloorUses = 8;
+
 int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir,
                        ErebusSolveStats *st) {
     int rc;
@@ -688,6 +692,7 @@ int band_solve_refined(erebus_state *s, BandSystem &sys, double rtol, int max_ir
         solves = 1;
     }
     bool first_check = true;
+    bool stalled = false, at_floor = false;
 refine:
     for (;;) {
         EREBUS_LAUNCH(s, k_band_residual, nblocks(np), kThreads, 0, B, sys.x, sys.r);
@@ -716,7 +721,18 @@ refine:
         }
         // refinement has reached the accuracy the factors allow: the last
         // correction did not halve the residual
-        if (solves > 0 && rel > 0.5 * prev) break;
+        if (solves > 0 && rel > 0.5 * prev) { stalled = true; break; }
+        // Within a factor 2 of the residual at which this system's refinement
+        // last stalled, one more correction could at most halve it, and
+        // refinement would stop after it.  Stop now, after at least one
+        // correction; every kFloorUses-th solve refines to the stall again, so
+        // the floor is measured afresh.
+        if (solves > 0 && sys.floor_rel > 0.0 && rel <= 2.0 * sys.floor_rel &&
+            sys.floor_uses < kFloorUses) {
+            sys.floor_uses++;
+            at_floor = true;
+            break;
+        }
         if (solves > max_ir) break;
         prev = rel;
         cudaMemcpyAsync(sys.d, sys.r, np * 8, cudaMemcpyDeviceToDevice, s->stream);
@@ -728,7 +744,7 @@ refine:
     // Mixed precision: when refinement with the FP32 factors stalls above the
     // target, factor this matrix again in FP64 and go on refining from the
     // current solution.
-    if (!(rel <= rtol) && !escalated && use_multifrontal(s) && mf_is_fp32(sys)) {
+    if (!(rel <= rtol) && !at_floor && !escalated && use_multifrontal(s) && mf_is_fp32(sys)) {
         escalated = true;
         timer_end(s, sys.ph_solve);
         timer_begin(s, sys.ph_factor);
@@ -738,6 +754,7 @@ refine:
         sys.fp64_refactorizations++;
         timer_begin(s, sys.ph_solve);
         prev = INFINITY;
+        stalled = false;
         if (!(rel < INFINITY)) {
             cudaMemsetAsync(sys.x, 0, np * 8, s->stream);
             cold = true;
@@ -745,6 +762,12 @@ refine:
         goto refine;
     }
     timer_end(s, sys.ph_solve);
+    if (rel <= rtol) {
+        sys.floor_rel = 0.0;
+    } else if (stalled) {
+        sys.floor_rel = rel;
+        sys.floor_uses = 0;
+    }
     sys.have_x = rel < 1e-6;   // good enough to start the next solve from
     sys.warm_ok = sys.have_x && (forced ? start_ok : solves == 0);
     if (st) {

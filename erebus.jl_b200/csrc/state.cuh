@@ -91,6 +91,9 @@ struct BandSystem {
     bool factored = false;
     bool have_x = false;           // x holds a converged solution
     bool warm_ok = false;          // the last solve's starting point already met the target
+    double floor_rel = 0.0;        // residual at which refinement last stalled above its
+                                   // target (0: none seen since it last reached the target)
+    int floor_uses = 0;            // solves accepted at that floor since it was measured
     int factorizations = 0;        // number of factorisations so far
     int fp64_refactorizations = 0; // FP64 factorisations after stalled FP32 refinement
     int ph_factor = -1, ph_solve = -1;   // timer phases of this system
