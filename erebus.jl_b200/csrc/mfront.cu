@@ -178,7 +178,7 @@ __device__ void mf_invert_tile(T *Tt, MmaSmem &S, int *err) {
     __syncthreads();
     regs_from_smem(P, a);
     __syncthreads();
-    tile_inverse2(a, S.vec, err);
+    tile_inverse(a, S.vec, err);
     regs_to_smem(P, a);
     __syncthreads();
     unstage_tile(Tt, P);
@@ -216,7 +216,7 @@ __device__ void mf_update_tile(const MfView &V, const MfFront &f, int I, int J, 
         __syncthreads();
         regs_from_smem(P, a);
         __syncthreads();
-        tile_inverse2(a, S.vec, err);
+        tile_inverse(a, S.vec, err);
         regs_to_smem(P, a);
         __syncthreads();
         unstage_tile(C, P);
