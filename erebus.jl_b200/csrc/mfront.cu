@@ -351,6 +351,9 @@ k_mf_factor(MfView V, unsigned int *bar, int *err) {
                 V, fb, fe, FS.km, [K](int Kt, int Mt) { return K < Kt ? Mt - K - 1 : 0; },
                 [&](const MfFront &f, int u) { mf_l_tile<T>(V, f, K + 1 + u, K, S); });
             grid_barrier(bar, err);
+            // the last step has no update tasks in any front (mf_nupd is 0 for
+            // K = Kt - 1); ktmax is the same in every CTA, so all skip it
+            if (K + 1 == ktmax) break;
             mf_for_tasks(
                 V, fb, fe, FS.km, [K](int Kt, int Mt) { return mf_nupd(Kt, Mt, K); },
                 [&](const MfFront &f, int u) {
