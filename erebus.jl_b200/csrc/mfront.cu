@@ -901,9 +901,12 @@ static std::vector<int> mf_level_modes(const MfPlan &P, int G) {
     return mode;
 }
 
-// Leaves of 16 nodes for the 6-unknown system (96 unknowns), 64 nodes for
-// the scalar ones, so that a leaf fills its 64-wide tiles.
-static int mf_leaf(int dofs) { return dofs >= 4 ? 16 : 64; }
+// Leaves of at most 32 nodes for the 6-unknown system (at 141 x 141 the
+// bisection stops at regions of 21-32 nodes: 126-192 unknowns, two or three
+// 64-wide pivot tiles), 64 nodes for the scalar ones.  Measured at 141 x 141 against 8, 16 and 24
+// nodes (Stokes-Darcy) and 32 and 128 (scalar): 16 -> 32 takes one tree
+// level off and the timestep from 10.24 to 9.97 ms.
+static int mf_leaf(int dofs) { return dofs >= 4 ? 32 : 64; }
 
 // Builds the plan of `sys` from the column pattern of its assembled ELL
 // matrix (on the device) and uploads it.

@@ -78,7 +78,7 @@ def stepped(pkg, oracle):
     return st, o
 
 
-@pytest.mark.parametrize("leaf", [4, 16, 64])
+@pytest.mark.parametrize("leaf", [4, 16, 32, 64])
 def test_hydromech_matches_superlu(mf, stepped, leaf):
     st, o = stepped
     A, b = o.hydromech_system(st.dt)
