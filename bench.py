@@ -423,7 +423,7 @@ def run_ours(args):
         # DRAM bytes per launch of the Stokes-Darcy factorisation from one ncu
         # capture of this workload (dram__bytes.sum.per_second x duration,
         # profiles/k_mf_factor_planetesimal_141.md); other workloads: none
-        traffic = 5.48e9 if (args.workload == WORKLOAD and solver == 0 and fp32 == 0) else None
+        traffic = 5.43e9 if (args.workload == WORKLOAD and solver == 0 and fp32 == 0) else None
         roof = {"bound": "fp64", "kernel": kname, "phase": "hydro_factor",
                 "achieved": tf, "peak": f64, "unit": "TFLOP/s", "frac": tf / f64,
                 "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.matmul)",
@@ -441,7 +441,7 @@ def run_ours(args):
                       "unit": "GB/s", "peak_source": src,
                       "frac": fh.solve_bytes / (solve_ms / 1000.0) / 1e9 / hbm,
                       "bytes_per_launch": fh.solve_bytes,
-                      "traffic": 0.83e9 if (args.workload == WORKLOAD and solver == 0 and
+                      "traffic": 0.80e9 if (args.workload == WORKLOAD and solver == 0 and
                                             fp32 == 0) else None,
                       "note": "factor bytes read per forward+backward solve over the "
                               "hydro_solve phase time per refinement solve"}
