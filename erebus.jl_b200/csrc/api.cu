@@ -241,6 +241,7 @@ int erebus_destroy(erebus_state *s) {
     if (!s) return EREBUS_EINVAL;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->post_graph) cudaGraphExecDestroy(s->post_graph);
     for (void *p : s->allocations) cudaFree(p);
     band_free(s->hydro);
     band_free(s->thermal);

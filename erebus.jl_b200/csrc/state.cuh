@@ -111,6 +111,11 @@ struct erebus_state {
     cudaStream_t stream = nullptr;
     int device = 0;
     int64_t launches = 0;
+    // the Stokes-Darcy post-processing sequence as a CUDA graph (stencils.cu),
+    // for the solution vector it was captured with
+    cudaGraphExec_t post_graph = nullptr;
+    const double *post_graph_S = nullptr;
+    int64_t post_graph_launches = 0;
     std::string last_error;
 
     // device memory

@@ -415,7 +415,7 @@ int bulk_viscosity(erebus_state *s) {
 // E:6754-6846 after the solve: unpack, Aphi, fluid velocities, dt limit,
 // stresses, Aphi again, symmetrize, nodal adjustment.  Leaves dt, ynpl and
 // the yielding error sum in the device scalars.
-int hydro_post(erebus_state *s, const double *S) {
+static int hydro_post_launch(erebus_state *s, const double *S) {
     int np = np_of(s), nb = nb_of(s);
     GridPtrs G = grid_ptrs(s);
     cudaMemsetAsync(s->dsc->maxabs, 0, sizeof(s->dsc->maxabs), s->stream);
@@ -435,6 +435,42 @@ int hydro_post(erebus_state *s, const double *S) {
     EREBUS_LAUNCH(s, k_nodal, nblocks(nb), kThreads, 0, s->p, s->g, G, s->dsc, s->dsc, dd);
     EREBUS_LAUNCH(s, k_sum_fixed, 1, 1024, 0, dd, nb, &s->dsc->sum_ddd);
     return check_cuda(s, cudaGetLastError(), "hydro_post");
+}
+
+// The post-processing of a Stokes-Darcy pass is a fixed sequence of 13
+// kernels and 2 memsets whose arguments (parameters, geometry, grid and
+// scratch buffers, all fixed at erebus_create) change only with the solution
+// vector S.  It runs right after the host has read the refinement's
+// residual, so launched one by one the GPU waits on the host's launch rate.
+// It is captured into a CUDA graph once per S and replayed with one launch.
+int hydro_post(erebus_state *s, const double *S) {
+    if (!s->post_graph || s->post_graph_S != S) {
+        if (s->post_graph) {
+            cudaGraphExecDestroy(s->post_graph);
+            s->post_graph = nullptr;
+        }
+        const int64_t l0 = s->launches;
+        int rc = check_cuda(s, cudaStreamBeginCapture(s->stream,
+                                                      cudaStreamCaptureModeThreadLocal),
+                            "hydro_post capture");
+        if (rc) return rc;
+        rc = hydro_post_launch(s, S);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        if (!rc) rc = check_cuda(s, e, "hydro_post capture");
+        if (!rc) rc = check_cuda(s, cudaGraphInstantiate(&s->post_graph, g, 0),
+                                 "hydro_post graph");
+        if (g) cudaGraphDestroy(g);
+        s->post_graph_launches = s->launches - l0;
+        s->launches = l0;
+        if (rc) {
+            s->post_graph = nullptr;
+            return rc;
+        }
+        s->post_graph_S = S;
+    }
+    s->launches += s->post_graph_launches;
+    return check_cuda(s, cudaGraphLaunch(s->post_graph, s->stream), "hydro_post");
 }
 
 int finalize_plastic(erebus_state *s, int rollback) {
