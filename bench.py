@@ -66,7 +66,7 @@ def config_dict(pkg, name, extra=None):
     c = pkg.CONFIGS[name]
     d = {"workload": name, "grid": "%dx%d basic nodes" % (c["N"], c["N"]),
          "markers_per_cell": "%dx%d" % (c["mpc"], c["mpc"]),
-         "l2": "inputs larger than L2: the Stokes-Darcy factor storage (1.6 GB at 141x141) "
+         "l2": "inputs larger than L2: the Stokes-Darcy factor storage (1.5 GB at 141x141) "
                "is written and read every timestep, and the marker arrays are streamed"}
     if extra:
         d.update(extra)
