@@ -155,7 +155,8 @@ class ErebusStepStats(Structure):
 class ErebusFactorStats(Structure):
     _fields_ = [
         ("direct_solver", c_int32), ("fronts", c_int32), ("levels", c_int32),
-        ("factorizations", c_int32), ("fp64_refactorizations", c_int32), ("reserved", c_int32),
+        ("factorizations", c_int32), ("fp64_refactorizations", c_int32),
+        ("krylov_iterations", c_int32),
         ("unknowns", c_int64), ("storage_bytes", c_int64),
         ("flops", c_double), ("solve_bytes", c_double),
     ]
@@ -174,6 +175,8 @@ class ErebusSolverOptions(Structure):
         ("hydro_rtol", c_double), ("thermal_rtol", c_double),
         ("gravity_rtol", c_double), ("max_refinements", c_int32),
         ("reuse_factors", c_int32), ("direct_solver", c_int32), ("factor_fp32", c_int32),
+        ("krylov", c_int32), ("precond_fp32", c_int32), ("krylov_restart", c_int32),
+        ("refactor_iterations", c_int32),
     ]
 
 

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liberebus_b200.so")
 SOURCES = ["api.cu", "markers.cu", "stencils.cu", "assemble.cu", "bandlu.cu", "mfront.cu",
-           "adjoint.cu"]
+           "adjoint.cu", "krylov.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -217,6 +217,10 @@ int erebus_default_solver_options(ErebusSolverOptions *o) {
     o->reuse_factors = 1;
     o->direct_solver = EREBUS_SOLVER_MULTIFRONTAL;
     o->factor_fp32 = 0;
+    o->krylov = 0;
+    o->precond_fp32 = 0;
+    o->krylov_restart = 30;
+    o->refactor_iterations = 8;
     return EREBUS_OK;
 }
 
@@ -406,6 +410,7 @@ int erebus_factor_stats(erebus_state *s, int32_t system, ErebusFactorStats *out)
     out->unknowns = sys.n;
     out->factorizations = sys.factorizations;
     out->fp64_refactorizations = sys.fp64_refactorizations;
+    out->krylov_iterations = sys.krylov_iterations;
     return EREBUS_OK;
 }
 
@@ -413,9 +418,18 @@ int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o) {
     if (!s || !o) return EREBUS_EINVAL;
     if (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL && o->direct_solver != EREBUS_SOLVER_BAND)
         return EREBUS_EINVAL;
+    if (o->krylov && (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL || o->factor_fp32 ||
+                      o->krylov_restart < 1 || o->krylov_restart > KRYLOV_MAX_RESTART ||
+                      o->refactor_iterations < 1))
+        return EREBUS_EINVAL;
     if (o->direct_solver != s->opt.direct_solver ||
-        (o->factor_fp32 != 0) != (s->opt.factor_fp32 != 0)) {   // stale factors
-        s->hydro.factored = s->thermal.factored = s->gravity.factored = false;
+        (o->factor_fp32 != 0) != (s->opt.factor_fp32 != 0) ||
+        (o->krylov != 0) != (s->opt.krylov != 0) ||
+        (o->precond_fp32 != 0) != (s->opt.precond_fp32 != 0)) {   // stale factors
+        for (BandSystem *b : {&s->hydro, &s->thermal, &s->gravity}) {
+            b->factored = false;
+            b->has_factor = false;
+        }
     }
     s->opt = *o;
     return EREBUS_OK;
@@ -675,6 +689,13 @@ static int read_scalars(erebus_state *s) {
 
 static double slot(const erebus_state *s, int k) { return s->hsc->maxabs[k]; }
 
+// One solve of an assembled system: direct LU plus FP64 refinement (the
+// plain path), or the mixed-precision Krylov mode.
+static int solve_system(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats *st) {
+    if (s->opt.krylov) return krylov_solve(s, sys, rtol, st);
+    return band_solve_refined(s, sys, rtol, s->opt.max_refinements, st);
+}
+
 extern "C" {
 
 int erebus_markers_to_nodes(erebus_state *s, double timesum) {
@@ -688,7 +709,7 @@ int erebus_gravity(erebus_state *s, ErebusSolveStats *st) {
     if (!s) return EREBUS_EINVAL;
     cudaSetDevice(s->device);
     TRY(assemble_system(s, SYS_GRAVITY));
-    TRY(band_solve_refined(s, s->gravity, s->opt.gravity_rtol, s->opt.max_refinements, st));
+    TRY(solve_system(s, s->gravity, s->opt.gravity_rtol, st));
     size_t np = (size_t)s->g.Nx1 * s->g.Ny1;
     TRY(check_cuda(s, cudaMemcpyAsync(s->grid[G_FI], s->gravity.x, np * 8,
                                       cudaMemcpyDeviceToDevice, s->stream), "FI"));
@@ -713,7 +734,7 @@ int erebus_hydromech_pass(erebus_state *s, double *dt, int32_t iplast, int32_t *
     TRY(bulk_viscosity(s));
     TRY(assemble_system(s, SYS_HYDRO));
     timer_end(s, PH_HYDRO_ASSEMBLE);
-    TRY(band_solve_refined(s, s->hydro, s->opt.hydro_rtol, s->opt.max_refinements, st));
+    TRY(solve_system(s, s->hydro, s->opt.hydro_rtol, st));
     timer_begin(s, PH_HYDRO_POST);
     TRY(hydro_post(s, s->hydro.x));
     timer_end(s, PH_HYDRO_POST);
@@ -749,7 +770,7 @@ int erebus_thermal_solve(erebus_state *s, double dt, int32_t timestep, double *m
     timer_begin(s, PH_THERMAL_ASSEMBLE);
     TRY(assemble_system(s, SYS_THERMAL));
     timer_end(s, PH_THERMAL_ASSEMBLE);
-    TRY(band_solve_refined(s, s->thermal, s->opt.thermal_rtol, s->opt.max_refinements, st));
+    TRY(solve_system(s, s->thermal, s->opt.thermal_rtol, st));
     TRY(thermal_post(s, s->thermal.x));
     TRY(read_scalars(s));
     s->last_maxDT = slot(s, X_DT);

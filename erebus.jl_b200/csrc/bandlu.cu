@@ -423,7 +423,6 @@ __global__ void k_band_apply(BandView B, const double *x, double *y) {
 // Sums of squares of a and b in a fixed order: NORM_BLOCKS blocks write
 // partial sums (block k takes the k-th contiguous chunk), then one block adds
 // them up in block order -> out[0], out[1].
-constexpr int NORM_BLOCKS = 296, NORM_THREADS = 256;   // norm_part holds 2 x 1024
 __global__ void k_norms2_part(const double *a, const double *b, int64_t n, double *part) {
     __shared__ double sa[NORM_THREADS], sb[NORM_THREADS];
     int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
@@ -548,6 +547,7 @@ static int band_tiles(erebus_state *s, BandSystem &sys) {
 
 int band_free(BandSystem &sys) {
     mf_release(sys);
+    krylov_free(sys);
     void *ps[] = {sys.tiles, sys.rscale, sys.rhs, sys.x, sys.r,
                   sys.d, sys.ell_vals, sys.ell_cols, sys.ell_prev, sys.changed,
                   sys.bar, sys.err};
@@ -572,7 +572,7 @@ static int coop_blocks(erebus_state *s, const void *func, int threads, size_t sm
     return want < maxb ? want : maxb;
 }
 
-static int lu_error(erebus_state *s, BandSystem &sys, const char *what) {
+int mf_check_error(erebus_state *s, BandSystem &sys, const char *what) {
     int h = 0;
     int rc = check_cuda(s, cudaMemcpyAsync(&h, sys.err, sizeof(int), cudaMemcpyDeviceToHost,
                                            s->stream), what);
@@ -702,7 +702,7 @@ refine:
                                            forced && first_check ? 32 : 16,
                                            cudaMemcpyDeviceToHost, s->stream), "norms");
         if (rc) return rc;
-        rc = lu_error(s, sys, "LU");
+        rc = mf_check_error(s, sys, "LU");
         if (rc) return rc;
         double rr = s->hsc->norms[0], bb = s->hsc->norms[1];
         rel = bb > 0.0 ? sqrt(rr / bb) : sqrt(rr);

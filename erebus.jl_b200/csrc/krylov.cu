@@ -1,0 +1,306 @@
+// krylov.cu -- mixed-precision Krylov solves with a lagged LU preconditioner.
+//
+// The reference solves its three linear systems with a sparse direct LU at
+// every call (UMFPACK through LinearSolve / `\`, src/Erebus.jl:6612,
+// E:6736-6748, E:6925).  The plain path of this library does the same with
+// the multifrontal LU plus FP64 iterative refinement (bandlu.cu).  This file
+// is the library's mixed-precision form of those solves:
+//
+//  * flexible GMRES (right preconditioned, restarted) in FP64: residuals,
+//    matrix products with the assembled rows, Gram-Schmidt (two passes) and
+//    the solution update are FP64;
+//  * the preconditioner is the multifrontal LU of an earlier matrix of the
+//    same system, applied from an FP32 copy of its FP64 factors when
+//    precond_fp32 is set (a triangular solve then reads half the bytes);
+//  * the factors are kept while the matrix changes, and computed again (in
+//    FP64) only when the previous solve of the system needed more than
+//    refactor_iterations iterations, or when a solve reaches three times that
+//    many without converging.
+//
+// Every reduction is summed in a fixed order (block partials, then the blocks
+// in order), so a solve is reproducible run to run.  The residual targets are
+// the plain path's (hydro_rtol and friends).
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "solver.cuh"
+
+namespace erebus {
+
+namespace {
+
+constexpr int KB = 296;   // blocks of the partial dot products (2 per SM)
+constexpr int KT = 256;
+constexpr int kFloorUses = 8;   // solves accepted at a measured residual floor
+
+// part[i * KB + b] = block b's share of dot(V_i, w), i < nv.  Block b takes
+// the b-th contiguous chunk; inside a block lanes stride by KT and the KT
+// lane sums are reduced in a fixed tree.
+__global__ void __launch_bounds__(KT) k_mdot_part(const double *__restrict__ V, int64_t ld,
+                                                  int nv, const double *__restrict__ w,
+                                                  int64_t n, double *__restrict__ part) {
+    __shared__ double red[KT / 32];
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = 0; i < nv; i++) {
+        const double *v = V + (int64_t)i * ld;
+        double acc = 0.0;
+        for (int64_t k = lo + threadIdx.x; k < hi; k += KT) acc = fma(v[k], w[k], acc);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) red[warp] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int q = 0; q < KT / 32; q++) t += red[q];
+            part[(int64_t)i * KB + blockIdx.x] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// out[i] = sum_b part[i * KB + b] in block order (one block per i); with
+// `acc`, acc[i] += out[i] as well.
+__global__ void __launch_bounds__(KT) k_mdot_sum(const double *__restrict__ part,
+                                                 double *__restrict__ out,
+                                                 double *__restrict__ acc) {
+    __shared__ double red[KT];
+    const int i = blockIdx.x;
+    red[threadIdx.x] = threadIdx.x < KB ? part[(int64_t)i * KB + threadIdx.x] : 0.0;
+    if (threadIdx.x + KT < KB) red[threadIdx.x] += part[(int64_t)i * KB + threadIdx.x + KT];
+    __syncthreads();
+    for (int off = KT / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[i] = red[0];
+        if (acc) acc[i] += red[0];
+    }
+}
+
+// w += sign * sum_i c_i V_i (i in increasing order), c on the device
+__global__ void k_maxpy(double *__restrict__ w, const double *__restrict__ V, int64_t ld,
+                        int nv, const double *__restrict__ c, double sign, int64_t n) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double s = 0.0;
+    for (int i = 0; i < nv; i++) s = fma(c[i], V[(int64_t)i * ld + k], s);
+    w[k] = fma(sign, s, w[k]);
+}
+
+// y = A x with the scaled rows (ELL)
+__global__ void k_ell_matvec(BandView B, const double *__restrict__ x, double *__restrict__ y) {
+    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= (int64_t)B.NB * B.nb) return;
+    double s = 0.0;
+    for (int k = 0; k < B.ell; k++) {
+        const int c = B.ell_cols[row * B.ell + k];
+        if (c >= 0) s = fma(B.ell_vals[row * B.ell + k], x[c], s);
+    }
+    y[row] = s;
+}
+
+__global__ void k_scale(double *__restrict__ dst, const double *__restrict__ src, double f,
+                        int64_t n) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[k] = src[k] * f;
+}
+
+int kalloc(erebus_state *s, BandSystem &sys, int m) {
+    if (sys.kbasis && sys.kdim >= m) return EREBUS_OK;
+    if (sys.kbasis) cudaFree(sys.kbasis);
+    if (sys.kwork) cudaFree(sys.kwork);
+    sys.kbasis = nullptr;
+    sys.kwork = nullptr;
+    const int64_t np = (int64_t)sys.NB * sys.nb;
+    cudaError_t e = cudaMalloc(&sys.kbasis, (size_t)(2 * m + 1) * np * sizeof(double));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&sys.kwork, (size_t)(KB * (m + 2) + 4 * (m + 2)) * sizeof(double));
+    if (e != cudaSuccess) {
+        s->last_error = std::string("krylov basis: ") + cudaGetErrorString(e);
+        return EREBUS_ENOMEM;
+    }
+    sys.kdim = m;
+    return EREBUS_OK;
+}
+
+// Factor the current matrix in FP64 (and make the FP32 copy the triangular
+// solves read when precond_fp32 is set).
+int refactor(erebus_state *s, BandSystem &sys) {
+    timer_end(s, sys.ph_solve);
+    timer_begin(s, sys.ph_factor);
+    int rc = mf_factor(s, sys, false);
+    if (!rc && s->opt.precond_fp32) rc = mf_convert_fp32(s, sys);
+    timer_end(s, sys.ph_factor);
+    timer_begin(s, sys.ph_solve);
+    return rc;
+}
+
+}  // namespace
+
+int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats *st) {
+    const int m = s->opt.krylov_restart;
+    const int thr = s->opt.refactor_iterations;
+    int rc = kalloc(s, sys, m);
+    if (rc) return rc;
+    const int64_t np = (int64_t)sys.NB * sys.nb;
+    double *V = sys.kbasis;                        // V_0 .. V_m
+    double *Z = sys.kbasis + (int64_t)(m + 1) * np;   // Z_0 .. Z_{m-1}
+    double *part = sys.kwork;                      // KB * (m + 2)
+    double *hd = part + (int64_t)KB * (m + 2);      // h column (m + 2)
+    double *h2 = hd + (m + 2);                     // second Gram-Schmidt pass
+    double *yd = h2 + (m + 2);                     // update coefficients
+    double *nd = yd + (m + 2);                     // |w|^2
+    BandView B = band_view(sys);
+    const int nb = nblocks(np);
+
+    timer_begin(s, sys.ph_solve);
+    if (!sys.has_factor || (!sys.factored && sys.last_iterations > thr)) {
+        rc = refactor(s, sys);
+        if (rc) return rc;
+    }
+    if (!sys.have_x) cudaMemsetAsync(sys.x, 0, np * 8, s->stream);
+
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hh(m + 2);
+    int total = 0;
+    double rel = INFINITY, prev_cycle = INFINITY, bnorm = 0.0;
+    bool stalled = false;
+    double *part2 = s->norm_part;
+    for (int cycle = 0;; cycle++) {
+        // true residual r = b - A x into V_0, and its norm with |b|
+        EREBUS_LAUNCH(s, k_band_residual, nb, kThreads, 0, B, sys.x, V);
+        EREBUS_LAUNCH(s, k_norms2_part, NORM_BLOCKS, NORM_THREADS, 0, V, sys.rhs, np, part2);
+        EREBUS_LAUNCH(s, k_norms2_sum, 1, NORM_THREADS, 0, part2, NORM_BLOCKS,
+                      &s->dsc->norms[0]);
+        rc = check_cuda(s, cudaMemcpyAsync(&s->hsc->norms[0], &s->dsc->norms[0], 16,
+                                           cudaMemcpyDeviceToHost, s->stream), "krylov norms");
+        if (!rc) rc = mf_check_error(s, sys, "krylov");
+        if (rc) return rc;
+        const double rr = s->hsc->norms[0], bb = s->hsc->norms[1];
+        bnorm = bb > 0.0 ? sqrt(bb) : 1.0;
+        rel = sqrt(rr) / bnorm;
+        if (rel <= rtol || rr == 0.0) break;
+        if (!(rel < INFINITY)) {
+            s->last_error = std::string(sys.name) + " krylov solve: non-finite residual";
+            return EREBUS_ENONFINITE;
+        }
+        if (cycle > 0 && rel > 0.5 * prev_cycle) {   // a whole cycle did not halve it
+            stalled = true;
+            break;
+        }
+        // within a factor 2 of the residual at which this system's solves last
+        // stalled above the target: accept (every kFloorUses-th solve runs to
+        // the stall again, so the floor is measured afresh)
+        if (total > 0 && sys.floor_rel > 0.0 && rel <= 2.0 * sys.floor_rel &&
+            sys.floor_uses < kFloorUses) {
+            sys.floor_uses++;
+            break;
+        }
+        if (total >= 3 * thr && !sys.factored) {      // lagged factors no longer pay
+            rc = refactor(s, sys);
+            if (rc) return rc;
+        }
+        if (total >= 40 * thr) break;
+        prev_cycle = rel;
+        const double beta = sqrt(rr);
+        EREBUS_LAUNCH(s, k_scale, nb, kThreads, 0, V, V, 1.0 / beta, np);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int j = 0;
+        for (; j < m; j++) {
+            double *Vj = V + (int64_t)j * np, *Zj = Z + (int64_t)j * np;
+            double *W = V + (int64_t)(j + 1) * np;
+            rc = check_cuda(s, cudaMemcpyAsync(Zj, Vj, np * 8, cudaMemcpyDeviceToDevice,
+                                               s->stream), "krylov copy");
+            if (!rc) rc = mf_solve(s, sys, Zj);
+            if (rc) return rc;
+            EREBUS_LAUNCH(s, k_ell_matvec, nb, kThreads, 0, B, Zj, W);
+            // classical Gram-Schmidt, twice
+            EREBUS_LAUNCH(s, k_mdot_part, KB, KT, 0, V, np, j + 1, W, np, part);
+            EREBUS_LAUNCH(s, k_mdot_sum, j + 1, KT, 0, part, hd, (double *)nullptr);
+            EREBUS_LAUNCH(s, k_maxpy, nb, kThreads, 0, W, V, np, j + 1, hd, -1.0, np);
+            EREBUS_LAUNCH(s, k_mdot_part, KB, KT, 0, V, np, j + 1, W, np, part);
+            EREBUS_LAUNCH(s, k_mdot_sum, j + 1, KT, 0, part, h2, hd);
+            EREBUS_LAUNCH(s, k_maxpy, nb, kThreads, 0, W, V, np, j + 1, h2, -1.0, np);
+            EREBUS_LAUNCH(s, k_mdot_part, KB, KT, 0, W, np, 1, W, np, part);
+            EREBUS_LAUNCH(s, k_mdot_sum, 1, KT, 0, part, nd, (double *)nullptr);
+            rc = check_cuda(s, cudaMemcpyAsync(hh.data(), hd, (j + 1) * 8,
+                                               cudaMemcpyDeviceToHost, s->stream), "krylov h");
+            if (!rc) rc = check_cuda(s, cudaMemcpyAsync(&hh[j + 1], nd, 8,
+                                                        cudaMemcpyDeviceToHost, s->stream),
+                                     "krylov h");
+            if (!rc) rc = check_cuda(s, cudaStreamSynchronize(s->stream), "krylov h");
+            if (rc) return rc;
+            total++;
+            const double wn = sqrt(hh[j + 1]);
+            // Givens rotations of the new Hessenberg column
+            for (int i = 0; i < j; i++) {
+                const double a = hh[i], b = hh[i + 1];
+                hh[i] = cs[i] * a + sn[i] * b;
+                hh[i + 1] = -sn[i] * a + cs[i] * b;
+            }
+            const double a = hh[j], d = std::hypot(a, wn);
+            cs[j] = d > 0.0 ? a / d : 1.0;
+            sn[j] = d > 0.0 ? wn / d : 0.0;
+            hh[j] = d;
+            for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = hh[i];
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            const double est = fabs(g[j + 1]) / bnorm;
+            if (!(wn > 0.0) || !(est < INFINITY)) { j++; break; }
+            EREBUS_LAUNCH(s, k_scale, nb, kThreads, 0, W, W, 1.0 / wn, np);
+            if (est <= 0.5 * rtol) { j++; break; }
+        }
+        if (j > m) j = m;
+        // y = R^{-1} g (upper triangular, j x j), x += Z y
+        for (int i = j - 1; i >= 0; i--) {
+            double t = g[i];
+            for (int c = i + 1; c < j; c++) t -= H[(size_t)i * m + c] * y[c];
+            y[i] = t / H[(size_t)i * m + i];
+        }
+        rc = check_cuda(s, cudaMemcpyAsync(yd, y.data(), j * 8, cudaMemcpyHostToDevice,
+                                           s->stream), "krylov y");
+        if (rc) return rc;
+        EREBUS_LAUNCH(s, k_maxpy, nb, kThreads, 0, sys.x, Z, np, j, yd, 1.0, np);
+        // the host vector y is read by the copy above before it is reused
+        rc = check_cuda(s, cudaStreamSynchronize(s->stream), "krylov update");
+        if (rc) return rc;
+    }
+    timer_end(s, sys.ph_solve);
+    sys.last_iterations = total;
+    sys.krylov_iterations += total;
+    sys.have_x = rel < 1e-6;
+    sys.warm_ok = false;
+    if (rel <= rtol) {
+        sys.floor_rel = 0.0;
+    } else if (stalled) {
+        sys.floor_rel = rel;
+        sys.floor_uses = 0;
+    }
+    if (st) {
+        st->iterations = total;
+        st->converged = rel <= rtol;
+        st->rel_residual = rel;
+    }
+    if (!(rel <= rtol) && !(rel < 1e-6)) {
+        char msg[160];
+        snprintf(msg, sizeof msg,
+                 "%s krylov solve did not reach tolerance: relative residual %.3e after %d "
+                 "iterations", sys.name, rel, total);
+        s->last_error = msg;
+        return EREBUS_ENOCONV;
+    }
+    return EREBUS_OK;
+}
+
+void krylov_free(BandSystem &sys) {
+    if (sys.kbasis) cudaFree(sys.kbasis);
+    if (sys.kwork) cudaFree(sys.kwork);
+    sys.kbasis = nullptr;
+    sys.kwork = nullptr;
+    sys.kdim = 0;
+}
+
+}  // namespace erebus

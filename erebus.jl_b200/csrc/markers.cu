@@ -1331,8 +1331,6 @@ __global__ void k_noalloc_tm(const int64_t *tm, int8_t *tm8, int n, int *err) {
 
 }  // namespace erebus
 
-#include <mutex>
-
 extern "C" int erebus_markers_to_nodes_noalloc(const ErebusParams *p,
                                                const ErebusMarkersDevice *md,
                                                int64_t marknum,
@@ -1356,23 +1354,22 @@ extern "C" int erebus_markers_to_nodes_noalloc(const ErebusParams *p,
         if (!q) return EREBUS_EINVAL;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream_);
 
-    // Set-up, once per device with that device current: the device address
-    // of the scratch array (its host-side name is only a stand-in).
-    static std::mutex mu;
-    static unsigned char *scratch_of[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EREBUS_ECUDA;
-    unsigned char *base;
+    // Set-up, with the calling device current: the device address of the
+    // scratch array (its host-side name is only a stand-in).  It is looked
+    // up on every call rather than cached, because the address can change
+    // when the device's primary context is torn down and created again
+    // (cudaDeviceReset); after the first call on a device the lookup is a
+    // host-side table read.
+    unsigned char *base = nullptr;
     {
-        std::lock_guard<std::mutex> lock(mu);
-        if (!scratch_of[dev]) {
-            void *ptr = nullptr;
-            if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
-                return EREBUS_ECUDA;
-            scratch_of[dev] = static_cast<unsigned char *>(ptr);
-        }
-        base = scratch_of[dev];
+        void *ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
+            return EREBUS_ECUDA;
+        base = static_cast<unsigned char *>(ptr);
     }
+    // A launch error left behind by an unrelated earlier call is cleared
+    // here, so that the check after this call's launches reports only its own.
+    (void)cudaGetLastError();
 
     // carve the scratch
     double *sums = reinterpret_cast<double *>(base);

@@ -58,6 +58,7 @@ struct MfView {
 struct MfDevice {
     MfPlan plan;
     bool fp32 = false;   // the current factors are the float ones
+    bool solve32 = false;   // solves read F32, an FP32 copy of the FP64 factors in F64
     MfFront *fr = nullptr;
     void *F64 = nullptr, *F32 = nullptr;   // front storage of each precision, on first use
     double *vec = nullptr;
@@ -819,7 +820,7 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
 static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
     MfView V;
     V.fr = D.fr;
-    V.F = D.fp32 ? D.F32 : D.F64;
+    V.F = (D.fp32 || D.solve32) ? D.F32 : D.F64;
     V.vec = D.vec;
     V.vars = D.vars;
     V.eamap = D.eamap;
@@ -846,6 +847,7 @@ void mf_release(BandSystem &sys) {
         if (p) cudaFree(p);
     delete D;
     sys.mf = nullptr;
+    sys.has_factor = false;
 }
 
 template <class T>
@@ -978,6 +980,7 @@ static int mf_factor_t(erebus_state *s, BandSystem &sys) {
         }
     }
     D.fp32 = sizeof(T) == 4;
+    D.solve32 = false;
     MfView V = mf_view(D, sys);
     int rc = check_cuda(s, cudaMemsetAsync(F, 0, D.plan.storage * sizeof(T), s->stream),
                         "mf zero");
@@ -1012,8 +1015,36 @@ int mf_factor(erebus_state *s, BandSystem &sys, bool fp32) {
     rc = fp32 ? mf_factor_t<float>(s, sys) : mf_factor_t<double>(s, sys);
     if (rc) return rc;
     sys.factored = true;
+    sys.has_factor = true;
     sys.factorizations++;
     return EREBUS_OK;
+}
+
+__global__ void k_f64_to_f32(const double *__restrict__ src, float *__restrict__ dst,
+                             long long n) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+        dst[k] = (float)src[k];
+}
+
+int mf_convert_fp32(erebus_state *s, BandSystem &sys) {
+    MfDevice *D = sys.mf;
+    if (!D || !D->F64 || D->fp32) {
+        s->last_error = "mf_convert_fp32: no FP64 factors";
+        return EREBUS_EINVAL;
+    }
+    if (!D->F32) {
+        cudaError_t e = cudaMalloc(&D->F32, D->plan.storage * sizeof(float));
+        if (e != cudaSuccess) {
+            D->F32 = nullptr;
+            s->last_error = std::string("multifrontal FP32 copy: ") + cudaGetErrorString(e);
+            return EREBUS_ENOMEM;
+        }
+    }
+    EREBUS_LAUNCH(s, k_f64_to_f32, 4 * mf_grid(s), 256, 0, (const double *)D->F64,
+                  (float *)D->F32, (long long)D->plan.storage);
+    D->solve32 = true;
+    return check_cuda(s, cudaGetLastError(), "mf_convert_fp32");
 }
 
 void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o) {
@@ -1032,9 +1063,11 @@ void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o
     o->fronts = (int32_t)P.fronts.size();
     o->levels = (int32_t)P.level_begin.size() - 1;
     const int es = s->opt.factor_fp32 ? sizeof(float) : sizeof(double);
+    const int ss = (s->opt.factor_fp32 || (s->opt.krylov && s->opt.precond_fp32))
+                       ? sizeof(float) : sizeof(double);
     o->storage_bytes = P.storage * (int64_t)es;
     o->flops = tiles * 2.0 * T2 * NB_TILE;
-    o->solve_bytes = rd * T2 * es;
+    o->solve_bytes = rd * T2 * ss;
 }
 
 int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
@@ -1045,7 +1078,8 @@ int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
     MfDevice &D = *sys.mf;
     MfView V = mf_view(D, sys);
     size_t smem = sizeof(MfSolveSmem);
-    const void *fn = D.fp32 ? (const void *)k_mf_solve<float> : (const void *)k_mf_solve<double>;
+    const void *fn = (D.fp32 || D.solve32) ? (const void *)k_mf_solve<float>
+                                           : (const void *)k_mf_solve<double>;
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int blocks = mf_blocks(s, fn, smem);
     if (blocks < 1) {

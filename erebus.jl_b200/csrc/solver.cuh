@@ -63,6 +63,22 @@ int mf_solve(erebus_state *s, BandSystem &sys, double *w);
 void mf_release(BandSystem &sys);
 void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o);
 void band_stats(const BandSystem &sys, ErebusFactorStats *o);
+// Residual and norm kernels of the refinement loop (bandlu.cu), shared with
+// the Krylov solves (krylov.cu).
+constexpr int NORM_BLOCKS = 296, NORM_THREADS = 256;   // norm_part holds 2 x 1024
+__global__ void k_band_residual(BandView B, const double *x, double *r);
+__global__ void k_norms2_part(const double *a, const double *b, int64_t n, double *part);
+__global__ void k_norms2_sum(const double *part, int nparts, double *out);
+// Reads the device error flag of the LU kernels (synchronises the stream).
+int mf_check_error(erebus_state *s, BandSystem &sys, const char *what);
+// An FP32 copy of the current FP64 multifrontal factors; later triangular
+// solves read the copy (until the next factorisation).
+int mf_convert_fp32(erebus_state *s, BandSystem &sys);
+// Mixed-precision Krylov mode (krylov.cu): flexible GMRES in FP64 with the
+// multifrontal LU of an earlier matrix as preconditioner.
+constexpr int KRYLOV_MAX_RESTART = 64;
+int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats *st);
+void krylov_free(BandSystem &sys);
 // true when `sys` is factored by the multifrontal LU (else the band LU)
 bool use_multifrontal(const erebus_state *s);
 int export_system(erebus_state *s, int kind, int64_t *nnz, int64_t *rows, int64_t *cols,

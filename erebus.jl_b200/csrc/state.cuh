@@ -97,6 +97,13 @@ struct BandSystem {
     int factorizations = 0;        // number of factorisations so far
     int fp64_refactorizations = 0; // FP64 factorisations after stalled FP32 refinement
     int ph_factor = -1, ph_solve = -1;   // timer phases of this system
+    // Krylov mode (krylov.cu)
+    bool has_factor = false;       // factors exist (possibly of an earlier matrix)
+    int krylov_iterations = 0;     // FGMRES iterations so far
+    int last_iterations = 0;       // iterations of this system's previous solve
+    int kdim = 0;                  // restart length the basis below was allocated for
+    double *kbasis = nullptr;      // V (kdim + 1 vectors) then Z (kdim vectors), np each
+    double *kwork = nullptr;       // dot partials, h, y (device)
 };
 
 }  // namespace erebus

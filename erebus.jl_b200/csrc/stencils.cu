@@ -443,6 +443,10 @@ static int hydro_post_launch(erebus_state *s, const double *S) {
 // vector S.  It runs right after the host has read the refinement's
 // residual, so launched one by one the GPU waits on the host's launch rate.
 // It is captured into a CUDA graph once per S and replayed with one launch.
+// The graph freezes every by-value argument (s->p, s->g, the grid pointers,
+// tmp_node, dsc).  That is correct only because none of them changes after
+// erebus_create: any future entry point that changes the parameters or
+// rebinds the grid must destroy s->post_graph so that it is captured again.
 int hydro_post(erebus_state *s, const double *S) {
     if (!s->post_graph || s->post_graph_S != S) {
         if (s->post_graph) {

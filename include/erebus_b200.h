@@ -183,10 +183,24 @@ typedef struct ErebusSolverOptions {
     int32_t reuse_factors;     /* 1: keep the LU factors while the scaled
                                   matrix is bitwise unchanged */
     int32_t direct_solver;     /* EREBUS_SOLVER_MULTIFRONTAL or EREBUS_SOLVER_BAND */
-    int32_t factor_fp32;       /* 1: mixed precision -- the multifrontal factors are
-                                  computed and stored in FP32 (tensor-core products
-                                  with three TF32 terms), residuals and refinement
-                                  stay FP64 */
+    int32_t factor_fp32;       /* 1: the multifrontal factors are computed and
+                                  stored in FP32 (tensor-core products with three
+                                  TF32 terms), residuals and refinement stay FP64 */
+    /* Mixed-precision Krylov mode (no reference counterpart; multifrontal
+       solver only).  With krylov = 1 each solve is a flexible GMRES in FP64
+       (residuals, matrix products, orthogonalisation, the solution update)
+       preconditioned by the multifrontal LU factors.  The factors are kept
+       as the preconditioner after the matrix changes and computed again (in
+       FP64) only when the previous solve of the system needed more than
+       refactor_iterations Krylov iterations, or when a solve reaches
+       3 x refactor_iterations without converging.  With precond_fp32 = 1 the
+       preconditioner is applied from an FP32 copy of those FP64 factors
+       (half the bytes per triangular solve).  The residual targets above
+       apply unchanged. */
+    int32_t krylov;            /* 1: FGMRES with lagged LU preconditioner */
+    int32_t precond_fp32;      /* 1: apply the preconditioner from FP32 factors */
+    int32_t krylov_restart;    /* FGMRES restart length (1..64) */
+    int32_t refactor_iterations; /* refresh the factors after a solve that took more */
 } ErebusSolverOptions;
 
 /* Size and work of one system's direct solver (diagnostics; no reference
@@ -204,7 +218,7 @@ typedef struct ErebusFactorStats {
     int32_t fp64_refactorizations; /* mixed precision: matrices factored again in
                                       FP64 because refinement with the FP32
                                       factors stalled */
-    int32_t reserved;
+    int32_t krylov_iterations; /* FGMRES iterations so far (krylov mode) */
     int64_t unknowns;
     int64_t storage_bytes;     /* factor storage */
     double  flops;             /* per factorisation */
@@ -420,8 +434,11 @@ typedef ErebusGridHost ErebusGridDevice;
    and tk1; other pointers of g may be NULL).  Scratch (the cell sort and
    the weighted sums) is a file-scope device array of about 6.4 MB that
    every GPU which loads the library keeps until the process exits.  The
-   call allocates nothing.  Its first call on a device looks up that
-   array's device address and should come before any stream capture.
+   call allocates nothing.  Every call looks up that array's device
+   address with the calling device current (the address is not cached,
+   since it can change if the device's context is reset); the first call on
+   a device also loads the library's device code there, so that first call
+   should come before any stream capture.
    marknum above EREBUS_NOALLOC_MAX_MARKERS or a grid with more than
    EREBUS_NOALLOC_MAX_NODES nodes returns EREBUS_ECAPACITY without
    launching anything; a marker type outside 1..3 returns EREBUS_EINVAL.

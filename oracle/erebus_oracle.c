@@ -26,6 +26,11 @@
 #include <string.h>
 #include "../include/erebus_b200.h"
 
+void oracle_thermodynamic_xfer(const ErebusParams *p, const ErebusSumsHost *s,
+                               ErebusGridHost *G);
+void oracle_melt_composition(const ErebusParams *p, const ErebusMarkersHost *M,
+                             int64_t marknum, ErebusGridHost *G, ErebusSumsHost *s);
+
 #define AT(A, rows, i, j) (A)[((int64_t)(j) - 1) * (rows) + ((i) - 1)]
 
 /* ------------------------------------------------------------------------ */
@@ -534,7 +539,16 @@ int oracle_thermochemical_reaction(const ErebusParams *p, ErebusMarkersHost *M,
             add_to_grid(s->WTPSUM, Ny1, i, j, w, 1.0);
         }
     }
-    /* compute_thermodynamic_xfer! (E:2208-2222) */
+    oracle_thermodynamic_xfer(p, s, G);
+    return 0;
+}
+
+/* compute_thermodynamic_xfer! (E:2208-2222): DMP, DHP at the P nodes from
+   the reaction's marker sums, zero where no marker reacted. */
+void oracle_thermodynamic_xfer(const ErebusParams *p, const ErebusSumsHost *s,
+                               ErebusGridHost *G) {
+    Geo g = geo(p);
+    size_t np = (size_t)g.Nx1 * g.Ny1;
     for (size_t k = 0; k < np; k++) {
         double wt = s->WTPSUM[k];
         if (wt > 0.0) {
@@ -544,7 +558,6 @@ int oracle_thermochemical_reaction(const ErebusParams *p, ErebusMarkersHost *M,
             G->DMP[k] = G->DHP[k] = 0.0;
         }
     }
-    return 0;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1224,6 +1237,18 @@ int oracle_nodes_to_markers(const ErebusParams *p, ErebusMarkersHost *M,
         M->phim[m] = jmax(p->phimin, jmin(p->phimax, ph / ((1.0 - ph) * exp(aphim * dt) + ph)));
     }
     memcpy(M->phinewm, M->phim, (size_t)marknum * 8);
+    oracle_melt_composition(p, M, marknum, G, s);
+    return 0;
+}
+
+/* update_p_nodes_melt_composition! (E:1929-1939, with E:1883 and E:2239):
+   XWsolidm0 scattered to the P nodes in marker order and normalised by the
+   weights, zero where no marker contributes. */
+void oracle_melt_composition(const ErebusParams *p, const ErebusMarkersHost *M,
+                             int64_t marknum, ErebusGridHost *G, ErebusSumsHost *s) {
+    Geo g = geo(p);
+    int Ny1 = g.Ny1;
+    size_t np = (size_t)g.Nx1 * Ny1;
     memset(s->XWSSUM, 0, np * 8);
     memset(s->WTPSUM, 0, np * 8);
     for (int64_t m = 0; m < marknum; m++) {
@@ -1235,7 +1260,6 @@ int oracle_nodes_to_markers(const ErebusParams *p, ErebusMarkersHost *M,
     }
     for (size_t k = 0; k < np; k++)
         G->XWS[k] = s->WTPSUM[k] > 0.0 ? s->XWSSUM[k] * (1.0 / s->WTPSUM[k]) : 0.0;
-    return 0;
 }
 
 /* ------------------------------------------------------------------------ */

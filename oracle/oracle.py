@@ -106,6 +106,8 @@ def lib():
             "oracle_insulating_bc": (None, [P, P]),
             "oracle_subgrid_stress": (I, [P, P, I64, P, P, D]),
             "oracle_subgrid_temperature": (I, [P, P, I64, P, P, D]),
+            "oracle_thermodynamic_xfer": (None, [P, P, P]),
+            "oracle_melt_composition": (None, [P, P, I64, P, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -120,6 +122,24 @@ def _p(x):
 
 def _a(arr):
     return arr.ctypes.data_as(ctypes.c_void_p)
+
+
+def finalize_thermochemical_iteration_pass(p, maxDT, dt, titer):
+    """finalize_thermochemical_iteration_pass (E:4187-4197): at the first
+    thermochemical iteration, dt shrinks so that the largest temperature
+    change is DTmax."""
+    if titer == 1 and maxDT > p.DTmax:
+        dt *= p.DTmax * (1.0 / maxDT)
+    return dt
+
+
+def thermochemical_iteration_outcome(p, DMP, pf, pf0, titer):
+    """compute_thermochemical_iteration_outcome (E:4216-4223): the
+    iteration stops once the fluid pressure changed by less than pferrmax
+    and either two iterations were taken or no marker reacted."""
+    pferr = float(np.max(np.abs(pf - pf0)))
+    dmpmax = float(np.max(np.abs(DMP)))
+    return pferr < p.pferrmax and (titer > 2 or dmpmax <= 0.0)
 
 
 class Oracle:
@@ -281,12 +301,11 @@ class Oracle:
                     break
             t0 = time.perf_counter()
             maxDT = self.thermal(dt, timestep)
-            if titer == 1 and maxDT > p.DTmax:       # E:4187-4197
-                dt *= p.DTmax * (1.0 / maxDT)
-            pferr = float(np.max(np.abs(grid["pf"] - grid["pf0"])))   # E:4216
-            dmpmax = float(np.max(np.abs(grid["DMP"])))
+            dt = finalize_thermochemical_iteration_pass(p, maxDT, dt, titer)
+            done = thermochemical_iteration_outcome(p, grid["DMP"], grid["pf"], grid["pf0"],
+                                                    titer)
             self._t("thermal", t0)
-            if pferr < p.pferrmax and (titer > 2 or dmpmax <= 0.0):
+            if done:
                 break
         t0 = time.perf_counter()
         L.oracle_nodes_to_markers(self.pP, self.pM, st.marknum, self.pG, self.pS,
