@@ -1,15 +1,21 @@
-"""Benchmark: MIC timesteps per second of the plain FP64 GPU path.
+"""Benchmark: MIC timesteps per second of the mixed-precision GPU path beside
+the plain FP64 GPU path.
 
-Workload (default): the synthetic 141x141 planetesimal (490,000 markers, 5x5
-per cell; 140 km box, 50 km rock body in sticky air; per-marker porosity
-U(0.05, 0.25) and log-uniform rock viscosity 1e18-1e20 Pa s).  A step is one
-whole timestep of simulation_loop (src/Erebus.jl:6370-7235).  With N GPUs
-(torchrun) every rank advances its own planetesimal (replicas; the path has
-no exchange step) and `value` is all ranks' timesteps over the slowest
+Workload (default): the synthetic 401x401 planetesimal (2,560,000 markers,
+4x4 per cell; 140 km box, 50 km rock body in sticky air; rock viscosity
+log-uniform per marker in 1e17-1e23 Pa s).  A step is one whole timestep of
+simulation_loop (src/Erebus.jl:6370-7235).  The line's `value` is the
+mixed-precision path (FGMRES in FP64 preconditioned by lagged multifrontal
+LU factors applied in FP32; ErebusSolverOptions.krylov); the plain FP64 path
+(direct LU of every new matrix plus FP64 refinement) is timed over the same
+timesteps from the same initial state and reported under "fp64", with the
+ratio.  Both solve every system to the same 1e-13 scaled residual.  With N
+GPUs (torchrun) every rank advances its own planetesimal (replicas; the path
+has no exchange step) and `value` is all ranks' timesteps over the slowest
 rank's device time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload planetesimal_401] [--direct-solver band]
+                    [--workload planetesimal_141] [--precision fp64|mixed]
 
 The line also carries "adjoint": gradients per second of the heat-path
 adjoint (20 timesteps forward and reversed, checkpoints every 5) on the
@@ -27,9 +33,12 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-METRIC = "MIC timesteps/sec (plain FP64 GPU path)"
+METRIC = "MIC timesteps/sec (mixed-prec vs FP64 GPU, rel err<=1e-8)"
 UNIT = "timesteps/s"
-WORKLOAD = "planetesimal_141"
+WORKLOAD = "planetesimal_401"
+# solver options of each precision mode (ErebusSolverOptions fields)
+MODES = {"fp64": {}, "mixed": {"krylov": 1, "precond_fp32": 1},
+         "fp32-factors": {"factor_fp32": 1}}
 
 
 def load_pkg():
@@ -66,8 +75,9 @@ def config_dict(pkg, name, extra=None):
     c = pkg.CONFIGS[name]
     d = {"workload": name, "grid": "%dx%d basic nodes" % (c["N"], c["N"]),
          "markers_per_cell": "%dx%d" % (c["mpc"], c["mpc"]),
-         "l2": "inputs larger than L2: the Stokes-Darcy factor storage (1.5 GB at 141x141) "
-               "is written and read every timestep, and the marker arrays are streamed"}
+         "l2": "inputs larger than L2: the Stokes-Darcy factor storage (GBs) is read by "
+               "every triangular solve and the marker arrays (>100 MB) are streamed every "
+               "timestep"}
     if extra:
         d.update(extra)
     return d
@@ -174,20 +184,43 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_baseline(pkg, O, name, steps=2):
-    """The oracle (C restatement + SuperLU) on the host cores: timestep 1
-    untimed, then `steps` timesteps timed."""
+def oracle_sample(pkg, O, name, steps, warmup):
+    """The oracle (C restatement of the reference's timestep with OpenMP on
+    the marker loops the reference threads, SuperLU solves) on the host
+    cores: `warmup` untimed timesteps, then `steps` timed ones.  Returns
+    (timesteps/s, seconds, first timed timestep)."""
     st = pkg.make_state(name)
     o = O.Oracle(st)
-    o.step(1)
+    for ts in range(1, warmup + 1):
+        o.step(ts)
     t0 = time.perf_counter()
-    for ts in range(2, 2 + steps):
+    for ts in range(warmup + 1, warmup + steps + 1):
         o.step(ts)
     el = time.perf_counter() - t0
-    return {"value": steps / el, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": "%s timesteps 2-%d of the same workload (timestep 1 untimed): OpenMP "
-                      "on the marker loops the reference threads, SuperLU direct solves, "
-                      "%.1f s" % (name, 1 + steps, el)}
+    return steps / el, el, warmup + 1
+
+
+def cpu_sample_plan(name):
+    """The bounded sample of a workload the CPU legs time: (timed steps,
+    warm-up steps, description).  At 401x401 one oracle timestep takes
+    minutes, so the sample is timestep 1 alone, which has one thermochemical
+    iteration where the timed GPU timesteps have three: the sample flatters
+    the CPU side."""
+    if name == "planetesimal_401":
+        return 1, 0, ("timestep 1 of the same workload (one thermochemical iteration; "
+                      "later timesteps take three, so this favours the CPU)")
+    if name == "planetesimal_141":
+        return 2, 1, "timesteps 2-3 of the same workload after 1 untimed"
+    return 3, 1, "timesteps 2-4 of the same workload after 1 untimed"
+
+
+def cpu_baseline(pkg, O, name):
+    steps, warm, what = cpu_sample_plan(name)
+    v, el, _ = oracle_sample(pkg, O, name, steps, warm)
+    return {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": "%s: oracle restatement of the reference (Julia is not available), "
+                      "OpenMP on the marker loops the reference threads, SuperLU direct "
+                      "solves with nested-dissection ordering, %.1f s" % (what, el)}
 
 
 def run_reference(args):
@@ -196,20 +229,10 @@ def run_reference(args):
         return 0
     pkg = load_pkg()
     O = load_oracle()
-    st = pkg.make_state(args.workload)
-    o = O.Oracle(st)
-    # each step is a bounded sample of the workload: the oracle needs about
-    # 10 s per 141x141 timestep on 16 cores, so the reference arm runs at
-    # most 2 timed steps after 1 untimed one
-    warm = min(args.warmup, 1)
-    steps = min(args.steps, 2)
-    for ts in range(1, warm + 1):
-        o.step(ts)
-    t0 = time.perf_counter()
-    for ts in range(warm + 1, warm + steps + 1):
-        o.step(ts)
-    el = time.perf_counter() - t0
-    v = steps / el
+    # each step is a bounded sample of the workload (cpu_sample_plan); the
+    # requested --steps / --warmup are recorded beside it
+    steps, warm, what = cpu_sample_plan(args.workload)
+    v, el, first = oracle_sample(pkg, O, args.workload, steps, warm)
     cores = os.cpu_count()
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
             "n_gpus": args.gpus, "steps": steps, "warmup": warm,
@@ -217,22 +240,19 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_dict(pkg, args.workload),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "timesteps %d-%d after %d untimed (requested %d "
-                                       "timed, %d warm-up), oracle restatement of the "
-                                       "reference (Julia is not available) with SuperLU "
-                                       "solves, OpenMP on the marker loops the reference "
-                                       "threads" % (warm + 1, warm + steps, warm, args.steps,
-                                                    args.warmup)},
+                             "sample": "%s (requested %d timed, %d warm-up); oracle "
+                                       "restatement of the reference (Julia is not "
+                                       "available) with SuperLU solves, OpenMP on the "
+                                       "marker loops the reference threads"
+                                       % (what, args.steps, args.warmup)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def algorithmic_bytes(st):
-    """Bytes each marker phase must move once (per launch of the phase)."""
-    g = st.g
-    n = st.marknum
-    nodes = g.Nx1 * g.Ny1
+def algorithmic_bytes(n, nodes):
+    """Bytes each marker phase must move once (per launch of the phase), for
+    n markers and `nodes` P nodes."""
     return {
         # read 16 marker fields (129 B) + write 7 derived (56 B); ~217 B per
         # P node of normalised outputs
@@ -339,22 +359,23 @@ def measure_ensemble(pkg, world, rank, bodies, steps, warmup, wave):
                        "precision": "fp64"}}
 
 
-def run_ours(args):
-    rank, world, local = dist_setup(args.gpus)
+def time_mode(pkg, args, mode, world, rank, local, clocks=False):
+    """One precision mode on the workload: `warmup` untimed timesteps, then
+    `steps` timed ones bracketed by a barrier and a device synchronisation,
+    timed with CUDA events on the library's stream (max over ranks), with
+    the device phase timer on."""
     import torch
-    pkg = load_pkg()
-    solver = {"multifrontal": 0, "band": 1}[args.direct_solver]
     st = pkg.make_state(args.workload)
-    fp32 = 1 if args.precision == "mixed" else 0
     sim = pkg.Simulation(st)
-    sim.set_solver_options(direct_solver=solver, factor_fp32=fp32)
+    sim.set_solver_options(**MODES[mode])
     for ts in range(1, args.warmup + 1):
         sim.step(ts)
+    f0 = {k: sim.factor_stats(i) for i, k in enumerate(("hydro", "thermal", "gravity"))}
     sim.enable_phase_timing(True)
     l0 = sim.kernel_launches()
     stream = torch.cuda.ExternalStream(sim.stream_handle())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clocks = Clocks(local) if rank == 0 else None
+    ck = Clocks(local) if clocks and rank == 0 else None
     barrier(world)
     torch.cuda.synchronize()
     e0.record(stream)
@@ -364,21 +385,82 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
-    ck = clocks.stop() if clocks else None
+    ck = ck.stop() if ck else None
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, world)
-    launches = sim.kernel_launches() - l0
-    phases = sim.phase_times()
-    fstats = {k: sim.factor_stats(i) for i, k in enumerate(("hydro", "thermal", "gravity"))}
-    value = world * args.steps / (ms_max / 1000.0)
-
-    # end to end through the public API: every step, the whole marker and
-    # grid state is uploaded from pinned host arrays, advanced and copied back
-    # (erebus_step_host; part of the copy-back overlaps the timestep)
-    st2 = pkg.make_state(args.workload).pinned()
+    out = {"ms": ms_max, "value": world * args.steps / (ms_max / 1000.0), "stats": stats,
+           "launches": sim.kernel_launches() - l0, "phases": sim.phase_times(),
+           "fstats": {k: sim.factor_stats(i)
+                      for i, k in enumerate(("hydro", "thermal", "gravity"))},
+           "clocks": ck, "marknum": st.marknum}
+    out["factorizations"] = {k: out["fstats"][k].factorizations - f0[k].factorizations
+                             for k in f0}
+    out["krylov_iterations"] = {k: out["fstats"][k].krylov_iterations -
+                                f0[k].krylov_iterations for k in f0}
     sim.close()
+    return out
+
+
+def phase_table(marknum, nodes, phases):
+    ab = algorithmic_bytes(marknum, nodes)
+    per = {}
+    for k, (t, c) in phases.items():
+        if c:
+            ent = {"ms_total": round(t, 3), "launches": c, "ms_per_launch": t / c}
+            if k in ab:
+                ent["GBps"] = ab[k] / (t / c / 1000.0) / 1e9
+            per[k] = ent
+    return per
+
+
+# DRAM traffic per launch of the dominant kernels, from ncu captures of the
+# same kernels (dram__bytes_read.sum + dram__bytes_write.sum).  Keyed by
+# (workload, kernel, factor precision); the profiles/ summaries give the
+# commands.  Absent entries are reported as null.
+NCU_TRAFFIC = {}
+
+
+def roofline(args, res, hbm, hbm_src, f64):
+    """Roofline of the headline mode's dominant kernel: the Stokes-Darcy
+    factorisation (k_mf_factor: FP64 tile flops against the DGEMM peak
+    measured in this run) or its triangular solves (k_mf_solve: factor bytes
+    read per solve against the measured HBM copy bandwidth), whichever takes
+    more device time."""
+    per, fh = res["per"], res["fstats"]["hydro"]
+    fac = per.get("hydro_factor", {}).get("ms_total", 0.0)
+    sol = per.get("hydro_precond", {}).get("ms_total", 0.0)
+    prec = "fp64" if args.precision == "fp64" else "fp32"
+    if fac >= sol and fac > 0:
+        ms = per["hydro_factor"]["ms_per_launch"]
+        tf = fh.flops / (ms / 1000.0) / 1e12
+        tr = NCU_TRAFFIC.get((args.workload, "k_mf_factor", "fp64"))
+        return {"bound": "fp64", "kernel": "k_mf_factor", "phase": "hydro_factor",
+                "achieved": tf, "peak": f64, "unit": "TFLOP/s", "frac": tf / f64,
+                "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.matmul)",
+                "traffic": tr, "flops_per_launch": fh.flops, "launches": per["hydro_factor"]["launches"],
+                "ms_per_launch": ms,
+                "note": "FP64 flops of the 64x64 tile algorithm (padding included) per "
+                        "factorisation over its event-timed duration"}
+    ms = per["hydro_precond"]["ms_per_launch"]
+    gbs = fh.solve_bytes / (ms / 1000.0) / 1e9
+    tr = NCU_TRAFFIC.get((args.workload, "k_mf_solve", prec))
+    return {"bound": "hbm", "kernel": "k_mf_solve", "phase": "hydro_precond",
+            "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+            "peak_source": hbm_src, "traffic": tr, "bytes_per_launch": fh.solve_bytes,
+            "launches": per["hydro_precond"]["launches"], "ms_per_launch": ms,
+            "note": "factor bytes one forward plus backward triangular solve reads (%s "
+                    "factors) over its event-timed duration" % prec}
+
+
+def measure_e2e(pkg, args, mode, world):
+    """End to end through the public API: every step, the whole marker and
+    grid state is uploaded from pinned host arrays, advanced one timestep and
+    copied back (erebus_step_host; part of the copy-back overlaps the
+    timestep)."""
+    import torch
+    st2 = pkg.make_state(args.workload).pinned()
     sim2 = pkg.Simulation(st2)
-    sim2.set_solver_options(direct_solver=solver, factor_fp32=fp32)
+    sim2.set_solver_options(**MODES[mode])
     for ts in range(1, 3):
         sim2.step(ts)
     sim2.download()
@@ -386,7 +468,6 @@ def run_ours(args):
         sum(a.nbytes for a in st2.grid.values())
     if st2.p.per_marker_eta:
         h2d += st2.m["etasolidm_m"][: st2.marknum].nbytes
-    d2h = h2d
     stream2 = torch.cuda.ExternalStream(sim2.stream_handle())
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ne2e = max(3, min(args.steps, 10))
@@ -394,83 +475,65 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2.record(stream2)
     for ts in range(3, 3 + ne2e):
-        sim2.step_host(ts)        # upload, timestep, copy-out (erebus_step_host)
+        sim2.step_host(ts)
     e3.record(stream2)
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
+    ms = max_over_ranks(e2.elapsed_time(e3), world)
     sim2.close()
+    return {"value": world * ne2e / (ms / 1000.0), "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(h2d), "steps": ne2e,
+            "precision": mode}
+
+
+def run_ours(args):
+    rank, world, local = dist_setup(args.gpus)
+    pkg = load_pkg()
+    head = args.precision
+    res = {}
+    for mode in (["fp64", head] if head != "fp64" else ["fp64"]):
+        res[mode] = time_mode(pkg, args, mode, world, rank, local, clocks=(mode == head))
+    e2e = measure_e2e(pkg, args, head, world)
     adj = None if args.no_adjoint else measure_adjoint(pkg, world)
     ens = None if args.no_ensemble else measure_ensemble(pkg, world, rank, 16, 5, 2, 16)
-    e2e = {"value": world * ne2e / (e2e_ms / 1000.0), "unit": UNIT,
-           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-           "steps": ne2e}
-
     if rank == 0:
         hbm, src = peaks()
         f64 = fp64_peak()
-        ab = algorithmic_bytes(st)
-        per = {}
-        for k, (t, c) in phases.items():
-            if c:
-                ent = {"ms_total": round(t, 3), "launches": c, "ms_per_launch": t / c}
-                if k in ab:
-                    ent["GBps"] = ab[k] / (t / c / 1000.0) / 1e9
-                per[k] = ent
-        dom = max(per, key=lambda k: per[k]["ms_total"])
-        fh = fstats["hydro"]
-        kname = "k_mf_factor" if solver == 0 else "k_band_factor"
-        tf = fh.flops / (per["hydro_factor"]["ms_per_launch"] / 1000.0) / 1e12
-        # DRAM bytes per launch of the Stokes-Darcy factorisation from one ncu
-        # capture of this workload (dram__bytes.sum.per_second x duration,
-        # profiles/k_mf_factor_planetesimal_141.md); other workloads: none
-        traffic = 5.43e9 if (args.workload == WORKLOAD and solver == 0 and fp32 == 0) else None
-        roof = {"bound": "fp64", "kernel": kname, "phase": "hydro_factor",
-                "achieved": tf, "peak": f64, "unit": "TFLOP/s", "frac": tf / f64,
-                "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.matmul)",
-                "traffic": traffic,
-                "traffic_source": "ncu capture, profiles/k_mf_factor_planetesimal_141.md"
-                                  if traffic else None,
-                "flops_per_launch": fh.flops,
-                "note": "dominant phase by device time: %s; FP64 flops of the 64x64 tile "
-                        "algorithm (padding included); DRAM traffic per launch is in the "
-                        "committed ncu summary" % dom}
-        solve_ms = per["hydro_solve"]["ms_per_launch"] / max(
-            1.0, sum(s.hydro_solves for s in stats) / max(1, sum(s.titer for s in stats)))
-        roof_solve = {"bound": "hbm", "kernel": "k_mf_solve" if solver == 0 else "k_band_solve",
-                      "achieved": fh.solve_bytes / (solve_ms / 1000.0) / 1e9, "peak": hbm,
-                      "unit": "GB/s", "peak_source": src,
-                      "frac": fh.solve_bytes / (solve_ms / 1000.0) / 1e9 / hbm,
-                      "bytes_per_launch": fh.solve_bytes,
-                      "traffic": 0.80e9 if (args.workload == WORKLOAD and solver == 0 and
-                                            fp32 == 0) else None,
-                      "note": "factor bytes read per forward+backward solve over the "
-                              "hydro_solve phase time per refinement solve"}
+        nodes = (pkg.CONFIGS[args.workload]["N"] + 1) ** 2
+        for mode, r in res.items():
+            r["per"] = phase_table(r["marknum"], nodes, r["phases"])
+        h = res[head]
+        roof = roofline(args, h, hbm, src, f64)
         cpu = None
-        if not args.no_cpu_baseline and args.workload == WORKLOAD:
+        if not args.no_cpu_baseline:
             cpu = cpu_baseline(pkg, load_oracle(), args.workload)
-        metric = METRIC if fp32 == 0 else \
-            "MIC timesteps/sec (mixed-precision GPU path: FP32 factors, FP64 refinement)"
-        line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world,
+        fp = res["fp64"]
+
+        def summary(mode, r):
+            return {"value": r["value"], "ms_per_step": r["ms"] / args.steps,
+                    "titer_per_step": [s.titer for s in r["stats"]],
+                    "factorizations": r["factorizations"],
+                    "krylov_iterations": r["krylov_iterations"],
+                    "hydro_solves": sum(s.hydro_solves for s in r["stats"]),
+                    "worst_rel_residual": max(s.worst_rel_residual for s in r["stats"]),
+                    "solver_options": MODES[mode], "phases": r["per"],
+                    "gpu_launches": r["launches"]}
+        line = {"metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "ms_per_step": h["ms"] / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if fp32 == 0 else "f64 (factors f32)", "data": "synthetic",
+                "dtype": "f64" if head == "fp64" else "f64 (preconditioner factors f32)",
+                "data": "synthetic",
                 "config": config_dict(pkg, args.workload,
                                       {"parallelism": "replicas x%d" % world,
-                                       "direct_solver": args.direct_solver,
-                                       "factor_precision": args.precision,
-                                       "titer_per_step": [s.titer for s in stats],
-                                       "hydro_solves": sum(s.hydro_solves for s in stats),
-                                       "thermal_solves": sum(s.thermal_solves for s in stats),
-                                       "gravity_solves": sum(s.gravity_solves for s in stats),
-                                       "factor_storage_GB": {k: v.storage_bytes / 1e9
-                                                             for k, v in fstats.items()},
-                                       "fp64_refactorizations": {
-                                           k: v.fp64_refactorizations
-                                           for k, v in fstats.items()}}),
-                "roofline": roof, "roofline_solve": roof_solve, "phases": per,
-                "cpu_baseline": cpu, "clocks": ck, "e2e": e2e, "gpu_launches": launches,
-                "adjoint": adj, "ensemble": ens}
+                                       "precision": head,
+                                       "solver_options": MODES[head],
+                                       "timesteps": [args.warmup + 1,
+                                                     args.warmup + args.steps]}),
+                "fp64": summary("fp64", fp),
+                "mixed_over_fp64": h["value"] / fp["value"],
+                "headline": summary(head, h),
+                "roofline": roof, "cpu_baseline": cpu, "clocks": h["clocks"], "e2e": e2e,
+                "gpu_launches": h["launches"], "adjoint": adj, "ensemble": ens}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -502,7 +565,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
-                    help="timed steps (default 50; ensemble workload: 20 per body)")
+                    help="timed steps (default 20; ensemble workload: 20 per body)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -517,9 +580,11 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=["planetesimal_41", "planetesimal_141", "planetesimal_401",
                              "ensemble"])
-    ap.add_argument("--direct-solver", default="multifrontal", choices=["multifrontal", "band"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
-                    help="mixed: FP32 multifrontal factors inside FP64 refinement")
+    ap.add_argument("--precision", default="mixed", choices=sorted(MODES),
+                    help="headline path: mixed (FGMRES with lagged FP32-applied LU "
+                         "preconditioner), fp64 (direct LU + FP64 refinement), or "
+                         "fp32-factors (FP32 factorisation + FP64 refinement); the FP64 "
+                         "path is always timed beside it")
     args = ap.parse_args()
     if args.impl == "reference" and args.workload == "ensemble":
         print(json.dumps({"impl": "reference", "unavailable": "the ensemble workload is "
@@ -528,7 +593,7 @@ def main():
         return 0
     if args.workload == "ensemble":
         return run_ensemble(args)
-    args.steps = args.steps or 50
+    args.steps = args.steps or 20
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -393,6 +393,7 @@ int erebus_create(const ErebusParams *p, int64_t marker_capacity, erebus_state *
         return fail(EREBUS_ENOMEM, "gravity system");
     s->hydro.ph_factor = PH_HYDRO_FACTOR;
     s->hydro.ph_solve = PH_HYDRO_SOLVE;
+    s->hydro.ph_precond = PH_HYDRO_PRECOND;
     s->thermal.ph_factor = PH_THERMAL_FACTOR;
     s->thermal.ph_solve = PH_THERMAL_SOLVE;
     if (cudaDeviceSynchronize() != cudaSuccess) return fail(EREBUS_ECUDA, "init");

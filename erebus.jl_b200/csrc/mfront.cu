@@ -1091,7 +1091,9 @@ int mf_solve(erebus_state *s, BandSystem &sys, double *w) {
     int epoch = ++D.epoch;
     void *args[] = {&V, &w, &bar, &err, &epoch};
     cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
+    timer_begin(s, sys.ph_precond);
     int rc = coop_launch(s, fn, blocks, LU_THREADS, args, smem, "mf_solve launch");
+    timer_end(s, sys.ph_precond);
     s->launches++;
     return rc;
 }

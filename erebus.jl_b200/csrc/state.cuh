@@ -97,6 +97,7 @@ struct BandSystem {
     int factorizations = 0;        // number of factorisations so far
     int fp64_refactorizations = 0; // FP64 factorisations after stalled FP32 refinement
     int ph_factor = -1, ph_solve = -1;   // timer phases of this system
+    int ph_precond = -1;                 // timer phase of its triangular solves
     // Krylov mode (krylov.cu)
     bool has_factor = false;       // factors exist (possibly of an earlier matrix)
     int krylov_iterations = 0;     // FGMRES iterations so far
@@ -193,7 +194,7 @@ enum Phase {
     PH_MARKERS_TO_NODES = 0, PH_GRAVITY, PH_REACTION, PH_HYDRO_ASSEMBLE,
     PH_HYDRO_FACTOR, PH_HYDRO_SOLVE, PH_HYDRO_POST, PH_THERMAL_ASSEMBLE,
     PH_THERMAL_FACTOR, PH_THERMAL_SOLVE, PH_NODES_TO_MARKERS, PH_RK4,
-    PH_BACKTRACE, PH_REPLENISH, PH_SCATTER_MERGE, PH_COUNT
+    PH_BACKTRACE, PH_REPLENISH, PH_SCATTER_MERGE, PH_HYDRO_PRECOND, PH_COUNT
 };
 void timer_begin(erebus_state *s, int phase);
 void timer_end(erebus_state *s, int phase);

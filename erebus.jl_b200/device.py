@@ -338,7 +338,7 @@ class Simulation:
     PHASES = ["markers_to_nodes", "gravity", "reaction", "hydro_assemble", "hydro_factor",
               "hydro_solve", "hydro_post", "thermal_assemble", "thermal_factor",
               "thermal_solve", "nodes_to_markers", "rk4", "backtrace", "replenish",
-              "scatter_merge"]
+              "scatter_merge", "hydro_precond"]
 
     def enable_phase_timing(self, on=True):
         self._check("erebus_enable_phase_timing",

@@ -407,7 +407,8 @@ int erebus_get_stream(const erebus_state *s, void **stream);
    reaction, Stokes-Darcy assembly, factorisation, triangular solves and
    refinement, post-solve stencils, heat assembly, factorisation, solves,
    nodes->markers, RK4 advection, pressure back-trace, replenishment,
-   scatter merge kernels.  Enabling resets the accumulators. */
+   scatter merge kernels, and the Stokes-Darcy triangular-solve launches
+   alone (inside the solve phase).  Enabling resets the accumulators. */
 int erebus_enable_phase_timing(erebus_state *s, int32_t on);
 int erebus_phase_times(erebus_state *s, double *ms, int64_t *counts, int32_t n);
 

@@ -201,8 +201,7 @@ class Oracle:
                                            _a(self.RT))
         return self._csc(n, self.coo_t, self.np), self.RT.copy()
 
-    @staticmethod
-    def solve(A, b):
+    def solve(self, A, b):
         """Direct solve with the rows scaled by their absolute sums first.
 
         This is the default row scaling of UMFPACK (UMFPACK_SCALE_SUM), the
@@ -210,11 +209,71 @@ class Oracle:
         E:6736-6748, E:6925).  Without it the Stokes-Darcy pressures at
         sticky-air nodes, whose rows carry coefficients ~1e-1 next to Darcy
         rows of ~1e23, are only determined to ~1e7 Pa by a backward-stable
-        solve and differ between orderings."""
+        solve and differ between orderings.
+
+        UMFPACK itself is not available; SuperLU (scipy.sparse.linalg.splu,
+        partial pivoting) stands in for it.  Its fill-reducing ordering is a
+        nested dissection of the node grid (recursive bisection of the node
+        rectangle by one-node-wide separators, all unknowns of a node kept
+        together), applied as a symmetric permutation with SuperLU's own
+        column ordering off: on these 2-D 9-point couplings it gives less
+        fill than COLAMD (48-58M against 73M factor entries at 201 x 201) and
+        halves the time.  As UMFPACK does by default (UMFPACK_IRSTEP = 2),
+        up to two steps of iterative refinement follow the solve."""
         rs = np.asarray(abs(A).sum(axis=1)).ravel()
         rs[rs == 0.0] = 1.0
         D = sp.diags(1.0 / rs)
-        return spla.splu((D @ A).tocsc(), permc_spec="COLAMD").solve(D @ b)
+        As = (D @ A).tocsc()
+        bs = D @ b
+        perm = self._nd_permutation(A.shape[0])
+        F = spla.splu(As[perm][:, perm].tocsc(), permc_spec="NATURAL")
+        x = np.empty_like(bs)
+        x[perm] = F.solve(bs[perm])
+        bn = np.linalg.norm(bs)
+        for _ in range(2):
+            r = bs - As @ x
+            if not np.linalg.norm(r) > 1e-15 * bn:
+                break
+            d = np.empty_like(bs)
+            d[perm] = F.solve(r[perm])
+            x += d
+        return x
+
+    def _nd_permutation(self, n):
+        """Unknown order of the nested dissection for a system of n unknowns
+        on the (Ny1, Nx1) P-node grid (n / nodes unknowns per node, node-major
+        as the assembly numbers them)."""
+        cache = self.__dict__.setdefault("_perms", {})
+        if n not in cache:
+            g = self.st.g
+            ny, nx = g.Ny1, g.Nx1
+            dof = n // (ny * nx)
+            order = []
+
+            def split(i0, i1, j0, j1):
+                h, w = i1 - i0, j1 - j0
+                if h <= 0 or w <= 0:
+                    return
+                if h * w <= 16:
+                    for j in range(j0, j1):
+                        order.extend(range(j * ny + i0, j * ny + i1))
+                    return
+                if w >= h:
+                    m = (j0 + j1) // 2
+                    split(i0, i1, j0, m)
+                    split(i0, i1, m + 1, j1)
+                    order.extend(range(m * ny + i0, m * ny + i1))
+                else:
+                    m = (i0 + i1) // 2
+                    split(i0, m, j0, j1)
+                    split(m + 1, i1, j0, j1)
+                    order.extend(j * ny + m for j in range(j0, j1))
+
+            split(0, ny, 0, nx)
+            nodes = np.asarray(order, dtype=np.int64)
+            assert nodes.size == ny * nx
+            cache[n] = (nodes[:, None] * dof + np.arange(dof)[None, :]).ravel()
+        return cache[n]
 
     # -- phases ----------------------------------------------------------------
     def markers_to_nodes(self, timesum):
