@@ -38,7 +38,7 @@ UNIT = "timesteps/s"
 WORKLOAD = "planetesimal_401"
 # solver options of each precision mode (ErebusSolverOptions fields)
 MODES = {"fp64": {}, "mixed": {"krylov": 1, "precond_fp32": 1},
-         "fp32-factors": {"factor_fp32": 1}}
+         "fp32-factors": {"factor_fp32": 1}, "krylov-fp64": {"krylov": 1}}
 
 
 def load_pkg():
@@ -585,7 +585,14 @@ def main():
                          "preconditioner), fp64 (direct LU + FP64 refinement), or "
                          "fp32-factors (FP32 factorisation + FP64 refinement); the FP64 "
                          "path is always timed beside it")
+    ap.add_argument("--refactor-iterations", type=int, default=None,
+                    help="Krylov modes: refresh the factors after a solve that took more "
+                         "iterations than this")
     args = ap.parse_args()
+    if args.refactor_iterations is not None:
+        for m in MODES.values():
+            if m.get("krylov"):
+                m["refactor_iterations"] = args.refactor_iterations
     if args.impl == "reference" and args.workload == "ensemble":
         print(json.dumps({"impl": "reference", "unavailable": "the ensemble workload is "
                           "timed on the GPU only; the CPU oracle takes ~10 s per 141x141 "

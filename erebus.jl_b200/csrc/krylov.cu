@@ -10,8 +10,9 @@
 //    matrix products with the assembled rows, Gram-Schmidt (two passes) and
 //    the solution update are FP64;
 //  * the preconditioner is the multifrontal LU of an earlier matrix of the
-//    same system, applied from an FP32 copy of its FP64 factors when
-//    precond_fp32 is set (a triangular solve then reads half the bytes);
+//    same system; with precond_fp32 set, the Stokes-Darcy system applies it
+//    from an FP32 copy of its FP64 factors (a triangular solve then reads
+//    half the bytes);
 //  * the factors are kept while the matrix changes, and computed again (in
 //    FP64) only when the previous solve of the system needed more than
 //    refactor_iterations iterations, or when a solve reaches three times that
@@ -126,13 +127,15 @@ int kalloc(erebus_state *s, BandSystem &sys, int m) {
     return EREBUS_OK;
 }
 
-// Factor the current matrix in FP64 (and make the FP32 copy the triangular
-// solves read when precond_fp32 is set).
+// Factor the current matrix in FP64 (and, for the Stokes-Darcy system when
+// precond_fp32 is set, make the FP32 copy its triangular solves read; the
+// scalar systems' solves are short, and their FP64 factors save the extra
+// iterations an FP32 copy costs).
 int refactor(erebus_state *s, BandSystem &sys) {
     timer_end(s, sys.ph_solve);
     timer_begin(s, sys.ph_factor);
     int rc = mf_factor(s, sys, false);
-    if (!rc && s->opt.precond_fp32) rc = mf_convert_fp32(s, sys);
+    if (!rc && s->opt.precond_fp32 && sys.dofs > 1) rc = mf_convert_fp32(s, sys);
     timer_end(s, sys.ph_factor);
     timer_begin(s, sys.ph_solve);
     return rc;
@@ -164,14 +167,15 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
     if (!sys.have_x) cudaMemsetAsync(sys.x, 0, np * 8, s->stream);
 
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hh(m + 2);
+    double *r = sys.r;                             // residual work vector
     int total = 0;
     double rel = INFINITY, prev_cycle = INFINITY, bnorm = 0.0;
     bool stalled = false;
     double *part2 = s->norm_part;
     for (int cycle = 0;; cycle++) {
-        // true residual r = b - A x into V_0, and its norm with |b|
-        EREBUS_LAUNCH(s, k_band_residual, nb, kThreads, 0, B, sys.x, V);
-        EREBUS_LAUNCH(s, k_norms2_part, NORM_BLOCKS, NORM_THREADS, 0, V, sys.rhs, np, part2);
+        // true residual r = b - A x, and its norm with |b|
+        EREBUS_LAUNCH(s, k_band_residual, nb, kThreads, 0, B, sys.x, r);
+        EREBUS_LAUNCH(s, k_norms2_part, NORM_BLOCKS, NORM_THREADS, 0, r, sys.rhs, np, part2);
         EREBUS_LAUNCH(s, k_norms2_sum, 1, NORM_THREADS, 0, part2, NORM_BLOCKS,
                       &s->dsc->norms[0]);
         rc = check_cuda(s, cudaMemcpyAsync(&s->hsc->norms[0], &s->dsc->norms[0], 16,
@@ -205,7 +209,7 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
         if (total >= 40 * thr) break;
         prev_cycle = rel;
         const double beta = sqrt(rr);
-        EREBUS_LAUNCH(s, k_scale, nb, kThreads, 0, V, V, 1.0 / beta, np);
+        EREBUS_LAUNCH(s, k_scale, nb, kThreads, 0, V, r, 1.0 / beta, np);
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
         int j = 0;

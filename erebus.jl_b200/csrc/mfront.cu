@@ -1063,7 +1063,8 @@ void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o
     o->fronts = (int32_t)P.fronts.size();
     o->levels = (int32_t)P.level_begin.size() - 1;
     const int es = s->opt.factor_fp32 ? sizeof(float) : sizeof(double);
-    const int ss = (s->opt.factor_fp32 || (s->opt.krylov && s->opt.precond_fp32))
+    const int ss = (s->opt.factor_fp32 ||
+                    (s->opt.krylov && s->opt.precond_fp32 && sys.dofs > 1))
                        ? sizeof(float) : sizeof(double);
     o->storage_bytes = P.storage * (int64_t)es;
     o->flops = tiles * 2.0 * T2 * NB_TILE;

@@ -194,9 +194,10 @@ typedef struct ErebusSolverOptions {
        FP64) only when the previous solve of the system needed more than
        refactor_iterations Krylov iterations, or when a solve reaches
        3 x refactor_iterations without converging.  With precond_fp32 = 1 the
-       preconditioner is applied from an FP32 copy of those FP64 factors
-       (half the bytes per triangular solve).  The residual targets above
-       apply unchanged. */
+       Stokes-Darcy preconditioner is applied from an FP32 copy of those FP64
+       factors (half the bytes per triangular solve); the heat and gravity
+       systems, whose solves are short, keep applying FP64 factors.  The
+       residual targets above apply unchanged. */
     int32_t krylov;            /* 1: FGMRES with lagged LU preconditioner */
     int32_t precond_fp32;      /* 1: apply the preconditioner from FP32 factors */
     int32_t krylov_restart;    /* FGMRES restart length (1..64) */

@@ -46,7 +46,8 @@ def main():
                     pre + "dt": stats["dt"], pre + "marknum": stats["marknum"],
                     pre + "seconds": el})
         for k in FIELDS:
-            out[pre + "grid_" + k] = np.asfortranarray(st.grid[k]).ravel(order="F")[::NODE_STRIDE]
+            out[pre + "grid_" + k] = np.array(
+                np.asfortranarray(st.grid[k]).ravel(order="F")[::NODE_STRIDE], copy=True)
         n = st.marknum
         for k in MARKER_FIELDS:
             out[pre + "m_" + k] = st.m[k][:n][::MARKER_STRIDE].copy()

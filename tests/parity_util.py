@@ -20,17 +20,18 @@ def rel_l2(a, b):
 
 
 def assert_step_parity(sg, so, gs, ostats, pos_tol=1e-10, field_tol=1e-8, res_tol=1e-10,
-                       what=""):
+                       dt_tol=1e-10, what=""):
     """One timestep of the device (state sg, ErebusStepStats gs) against the
     oracle (state so, its stats dict): the iteration counts and marker
-    population exactly, dt to 1e-10, marker positions to `pos_tol` relative
-    (max norm), marker temperature, porosity and water content to
-    `field_tol`, the solution fields to `field_tol` relative L2, and every
-    solve's final scaled residual to `res_tol`."""
-    assert gs.titer == ostats["titer"], what
-    assert gs.iplast_total == ostats["iplast_total"], what
-    assert gs.marknum == ostats["marknum"] == sg.marknum, what
-    assert abs(gs.dt - ostats["dt"]) <= 1e-10 * ostats["dt"], what
+    population exactly, dt to `dt_tol` relative, marker positions to
+    `pos_tol` relative (max norm), marker temperature, porosity and water
+    content to `field_tol`, the solution fields to `field_tol` relative L2,
+    and every solve's final scaled residual to `res_tol`."""
+    assert gs.titer == ostats["titer"], (what, gs.titer, ostats["titer"])
+    assert gs.iplast_total == ostats["iplast_total"], (what, gs.iplast_total,
+                                                      ostats["iplast_total"])
+    assert gs.marknum == ostats["marknum"] == sg.marknum, (what, gs.marknum, ostats["marknum"])
+    assert abs(gs.dt - ostats["dt"]) <= dt_tol * ostats["dt"], (what, gs.dt, ostats["dt"])
     assert gs.worst_rel_residual <= res_tol, (what, gs.worst_rel_residual)
     n = so.marknum
     for k in ["xm", "ym"]:

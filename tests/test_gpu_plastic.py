@@ -9,8 +9,10 @@ the roll-back period dtstep to 3, on the 41 x 41 workload: nodes yield
 error YERRNOD falls below yerrmax (E:4091), and every third pass halves dt
 and restores ETA00 / YNY00 (finalize_plastic_iteration_pass!, E:4142-4169).
 Each timestep is compared with the oracle's from the same input state: the
-number of thermochemical and plastic iterations exactly, dt to 1e-10, the
-solution fields to 1e-8 and marker positions to 1e-10.  The device adds the
+number of thermochemical and plastic iterations exactly, the solution fields
+to 1e-8, marker positions to 1e-10, and dt to 1e-8 (with yielding, dt is set
+by the displacement limit from the largest velocity, so it carries the
+solution's tolerance).  The device adds the
 squared yield errors in a different order from the serial oracle
 (k_sum_fixed), so YERRNOD agrees to rounding only; the iteration counts
 agreeing shows that no convergence decision flipped.
@@ -60,7 +62,9 @@ def test_plastic_iterations_match_oracle(pkg, oracle, built_lib, mode):
         ostats = o.step(ts)
         gs = sim.step(ts)
         sim.download()
-        assert_step_parity(sg, so, gs, ostats, what="%s timestep %d" % (mode, ts))
+        # dt is set by the displacement limit (E:3777-3803) from the largest
+        # velocities of the solution, which agree to the solution tolerance
+        assert_step_parity(sg, so, gs, ostats, dt_tol=1e-8, what="%s timestep %d" % (mode, ts))
         passes += ostats["iplast_total"]
         titers += ostats["titer"]
         for k in so.m:
