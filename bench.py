@@ -541,6 +541,50 @@ def run_ours(args):
     return 0
 
 
+def run_marker_phases(args):
+    """bench.py --marker-phases K: the marker phases alone on the workload's
+    initial state (no linear solve, so no factor storage is allocated; a
+    small device footprint for profiling), K rounds of markers_to_nodes,
+    the reaction, nodes_to_markers and RK4 advection under a synthetic rigid
+    rotation of the grid (about one cell per timestep at the box edge, so
+    the markers move and are sorted again every round).  Prints per-phase
+    device times and algorithmic GB/s."""
+    rank, world, local = dist_setup(args.gpus)
+    import torch
+    pkg = load_pkg()
+    st = pkg.make_state(args.workload)
+    g, p = st.g, st.p
+    dt = p.dt_longest
+    om = g.dx / (0.5 * p.xsize) / dt
+    ny1, nx1 = g.Ny1, g.Nx1
+    xs_vx = np.arange(nx1) * g.dx
+    ys_vx = -g.dy / 2 + np.arange(ny1) * g.dy
+    xs_vy = -g.dx / 2 + np.arange(nx1) * g.dx
+    ys_vy = np.arange(ny1) * g.dy
+    st.grid["vx"][...] = -om * (ys_vx[:, None] - g.ycenter) + 0 * xs_vx[None, :]
+    st.grid["vy"][...] = om * (xs_vy[None, :] - g.xcenter) + 0 * ys_vy[:, None]
+    st.grid["vxf"][...] = st.grid["vx"]
+    st.grid["vyf"][...] = st.grid["vy"]
+    st.grid["tk2"][...] = p.tkm0[0]
+    sim = pkg.Simulation(st)
+    sim.enable_phase_timing(True)
+    torch.cuda.synchronize()
+    for k in range(args.marker_phases):
+        ts = 2 + k
+        sim.markers_to_nodes(st.timesum)
+        sim.thermochemical_reaction(dt, ts, 1)
+        sim.nodes_to_markers(dt, ts)
+        sim.advect_rk4(dt)
+    torch.cuda.synchronize()
+    ph = sim.phase_times()
+    sim.close()
+    if rank == 0:
+        per = phase_table(st.marknum, g.Nx1 * g.Ny1, ph)
+        print(json.dumps({"workload": args.workload, "markers": st.marknum,
+                          "rounds": args.marker_phases, "phases": per}), flush=True)
+    return 0
+
+
 def run_ensemble(args):
     """bench.py --workload ensemble: the ensemble line alone (default 256
     bodies, 20 timed timesteps each after 3 untimed ones, 32 bodies at a
@@ -588,7 +632,11 @@ def main():
     ap.add_argument("--refactor-iterations", type=int, default=None,
                     help="Krylov modes: refresh the factors after a solve that took more "
                          "iterations than this")
+    ap.add_argument("--marker-phases", type=int, default=0,
+                    help="run only the marker phases this many times (profiling)")
     args = ap.parse_args()
+    if args.marker_phases:
+        return run_marker_phases(args)
     if args.refactor_iterations is not None:
         for m in MODES.values():
             if m.get("krylov"):
