@@ -629,6 +629,8 @@ __device__ __forceinline__ void mf_wait_flag(const int *flag, int want, int *err
         unsigned long long t0 = 0;
         for (int spin = 0;; spin++) {
             if (*(volatile const int *)flag >= want) break;
+            // once a wait of this launch has given up, the launch ends quickly
+            if (*(volatile const int *)err) break;
             if (spin == 0) {
                 t0 = globaltimer();
             } else if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
