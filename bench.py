@@ -378,12 +378,14 @@ def time_mode(pkg, args, mode, world, rank, local, clocks=False):
     ck = Clocks(local) if clocks and rank == 0 else None
     barrier(world)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed:" + mode)   # lets ncu capture the timed region alone
     e0.record(stream)
     stats = []
     for ts in range(args.warmup + 1, args.warmup + args.steps + 1):
         stats.append(sim.step(ts))
     e1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     barrier(world)
     ck = ck.stop() if ck else None
     ms = e0.elapsed_time(e1)
@@ -414,10 +416,17 @@ def phase_table(marknum, nodes, phases):
 
 
 # DRAM traffic per launch of the dominant kernels, from ncu captures of the
-# same kernels (dram__bytes_read.sum + dram__bytes_write.sum).  Keyed by
+# same kernels (dram__bytes_read.sum + dram__bytes_write.sum), keyed by
 # (workload, kernel, factor precision); the profiles/ summaries give the
 # commands.  Absent entries are reported as null.
-NCU_TRAFFIC = {}
+NCU_TRAFFIC = {
+    ("planetesimal_141", "k_mf_factor", "fp64"): 5.43e9,
+}
+# The triangular solve reads every factor tile once, so its traffic grows with
+# the factor bytes: captured at 141x141 (k_mf_solve<double>: 0.80 GB against
+# 0.79 GB of factors; k_mf_solve<float>: 0.409 GB against 0.430 GB), the
+# ratio scales the factor bytes of any workload to a per-launch figure.
+NCU_SOLVE_TRAFFIC_RATIO = {"fp64": 0.80 / 0.79, "fp32": 0.409 / 0.430}
 
 
 def roofline(args, res, hbm, hbm_src, f64):
@@ -443,10 +452,13 @@ def roofline(args, res, hbm, hbm_src, f64):
                         "factorisation over its event-timed duration"}
     ms = per["hydro_precond"]["ms_per_launch"]
     gbs = fh.solve_bytes / (ms / 1000.0) / 1e9
-    tr = NCU_TRAFFIC.get((args.workload, "k_mf_solve", prec))
+    tr = NCU_SOLVE_TRAFFIC_RATIO[prec] * fh.solve_bytes
     return {"bound": "hbm", "kernel": "k_mf_solve", "phase": "hydro_precond",
             "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
-            "peak_source": hbm_src, "traffic": tr, "bytes_per_launch": fh.solve_bytes,
+            "peak_source": hbm_src, "traffic": tr,
+            "traffic_source": "ncu capture at 141x141, DRAM bytes / factor bytes "
+                              "scaled to this launch's factor bytes",
+            "bytes_per_launch": fh.solve_bytes,
             "launches": per["hydro_precond"]["launches"], "ms_per_launch": ms,
             "note": "factor bytes one forward plus backward triangular solve reads (%s "
                     "factors) over its event-timed duration" % prec}
@@ -634,9 +646,17 @@ def main():
                          "iterations than this")
     ap.add_argument("--marker-phases", type=int, default=0,
                     help="run only the marker phases this many times (profiling)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the multifrontal analysis parameters for the workload by "
+                         "timing (erebus_b200.autotune); prints the trials as JSON")
     args = ap.parse_args()
     if args.marker_phases:
         return run_marker_phases(args)
+    if args.autotune:
+        load_pkg()
+        from erebus_b200 import autotune
+        prec = "mixed" if args.precision == "mixed" else "fp64"
+        return autotune.main(["--workload", args.workload, "--precision", prec])
     if args.refactor_iterations is not None:
         for m in MODES.values():
             if m.get("krylov"):

@@ -176,7 +176,9 @@ class ErebusSolverOptions(Structure):
         ("gravity_rtol", c_double), ("max_refinements", c_int32),
         ("reuse_factors", c_int32), ("direct_solver", c_int32), ("factor_fp32", c_int32),
         ("krylov", c_int32), ("precond_fp32", c_int32), ("krylov_restart", c_int32),
-        ("refactor_iterations", c_int32),
+        ("refactor_iterations", c_int32), ("mf_leaf_vector", c_int32),
+        ("mf_leaf_scalar", c_int32), ("mf_local_factor_ops", c_int32),
+        ("mf_local_solve_tiles", c_int32),
     ]
 
 

@@ -221,6 +221,10 @@ int erebus_default_solver_options(ErebusSolverOptions *o) {
     o->precond_fp32 = 0;
     o->krylov_restart = 30;
     o->refactor_iterations = 8;
+    o->mf_leaf_vector = 0;
+    o->mf_leaf_scalar = 0;
+    o->mf_local_factor_ops = 0;
+    o->mf_local_solve_tiles = 0;
     return EREBUS_OK;
 }
 
@@ -419,10 +423,22 @@ int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o) {
     if (!s || !o) return EREBUS_EINVAL;
     if (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL && o->direct_solver != EREBUS_SOLVER_BAND)
         return EREBUS_EINVAL;
+    if (o->mf_leaf_vector < 0 || o->mf_leaf_scalar < 0 || o->mf_local_factor_ops < 0 ||
+        o->mf_local_solve_tiles < 0)
+        return EREBUS_EINVAL;
     if (o->krylov && (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL || o->factor_fp32 ||
                       o->krylov_restart < 1 || o->krylov_restart > KRYLOV_MAX_RESTART ||
                       o->refactor_iterations < 1))
         return EREBUS_EINVAL;
+    if (o->mf_leaf_vector != s->opt.mf_leaf_vector ||
+        o->mf_leaf_scalar != s->opt.mf_leaf_scalar ||
+        o->mf_local_factor_ops != s->opt.mf_local_factor_ops ||
+        o->mf_local_solve_tiles != s->opt.mf_local_solve_tiles) {   // analysed again
+        for (BandSystem *b : {&s->hydro, &s->thermal, &s->gravity}) {
+            mf_release(*b);
+            b->factored = false;
+        }
+    }
     if (o->direct_solver != s->opt.direct_solver ||
         (o->factor_fp32 != 0) != (s->opt.factor_fp32 != 0) ||
         (o->krylov != 0) != (s->opt.krylov != 0) ||
@@ -553,9 +569,6 @@ int erebus_snapshot_begin(erebus_state *s, const ErebusGridHost *gh,
     if (s->snap_cap < need) {
         if (s->snap_dev) cudaFree(s->snap_dev);
         if (s->snap_tm) cudaFreeHost(s->snap_tm);
-    if (s->tm64) cudaFree(s->tm64);
-    if (s->ev_to_coop) cudaEventDestroy(s->ev_to_coop);
-    if (s->ev_from_coop) cudaEventDestroy(s->ev_from_coop);
         s->snap_dev = nullptr;
         s->snap_tm = nullptr;
         s->snap_cap = 0;

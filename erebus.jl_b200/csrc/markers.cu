@@ -983,7 +983,11 @@ __device__ __forceinline__ double vy_at(const Geo &g, const double *v, double x,
     return (1.0 - dxmj / dx) * v12 + (dxmj / dx) * v34;
 }
 
-__global__ void k_rk4(ErebusParams p, Geo g, MP M, GPtr G, int n, double dt) {
+// 7 blocks of 128 threads per SM (72 registers a thread, against 84 and 6
+// blocks unbounded): the kernel is bound by the latency of its FP64
+// divisions and gathers, so it wants warps in flight more than registers.
+__global__ void __launch_bounds__(128, 7)
+k_rk4(ErebusParams p, Geo g, MP M, GPtr G, int n, double dt) {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= n) return;
     const double B[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
@@ -996,7 +1000,9 @@ __global__ void k_rk4(ErebusParams p, Geo g, MP M, GPtr G, int n, double dt) {
     grid_weights(g, GB, xmm, ymm, i, j, w);
     double om = gather4(G.f[G_wyx], Ny, i, j, w);
     double th = dt * om;
-    double c = cos(th), sn = sin(th), s2 = sin(2.0 * th), c2 = cos(2.0 * th);
+    double c, sn, s2, c2;
+    sincos(th, &sn, &c);
+    sincos(2.0 * th, &s2, &c2);
     double sxx = M.f[M_sxxm][m], sxy = M.f[M_sxym][m];
     M.f[M_sxxm][m] = sxx * (c * c) - sxx * (sn * sn) - sxy * s2;
     M.f[M_sxym][m] = sxx * s2 + sxy * c2;

@@ -876,7 +876,8 @@ static int mf_grid(erebus_state *s) {
 // thresholds come from timing each phase of the 141x141 systems on a B200.
 constexpr int kLocalFactorOps = 8;    // tile operations per CTA
 constexpr int kLocalSolveTiles = 24;  // tiles streamed per CTA and sweep
-static std::vector<int> mf_level_modes(const MfPlan &P, int G) {
+static std::vector<int> mf_level_modes(const MfPlan &P, int G, int factor_ops,
+                                       int solve_tiles) {
     std::vector<int> mode;
     for (size_t p = 0; p + 1 < P.level_begin.size(); p++) {
         const int fb = P.level_begin[p], fe = P.level_begin[p + 1], F = fe - fb;
@@ -898,8 +899,8 @@ static std::vector<int> mf_level_modes(const MfPlan &P, int G) {
         }
         const bool forced = F >= G / 2 || F > MF_KM_MAX;
         int m = 0;
-        if (forced || waves * ops <= kLocalFactorOps) m |= MF_FACTOR_LOCAL;
-        if (forced || waves * tiles <= kLocalSolveTiles) m |= MF_SOLVE_LOCAL;
+        if (forced || waves * ops <= factor_ops) m |= MF_FACTOR_LOCAL;
+        if (forced || waves * tiles <= solve_tiles) m |= MF_SOLVE_LOCAL;
         mode.push_back(m);
     }
     return mode;
@@ -910,7 +911,10 @@ static std::vector<int> mf_level_modes(const MfPlan &P, int G) {
 // 64-wide pivot tiles), 64 nodes for the scalar ones.  Measured at 141 x 141 against 8, 16 and 24
 // nodes (Stokes-Darcy) and 32 and 128 (scalar): 16 -> 32 takes one tree
 // level off and the timestep from 10.24 to 9.97 ms.
-static int mf_leaf(int dofs) { return dofs >= 4 ? 32 : 64; }
+static int mf_leaf(const erebus_state *s, int dofs) {
+    const int o = dofs >= 4 ? s->opt.mf_leaf_vector : s->opt.mf_leaf_scalar;
+    return o > 0 ? o : dofs >= 4 ? 32 : 64;
+}
 
 // Builds the plan of `sys` from the column pattern of its assembled ELL
 // matrix (on the device) and uploads it.
@@ -925,7 +929,7 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
     if (!rc) rc = check_cuda(s, cudaStreamSynchronize(s->stream), "mf pattern");
     if (rc) return rc;
     MfPlan &P = D->plan;
-    if (!mf_analyse(P, dofs, s->g.Ny1, s->g.Nx1, mf_leaf(dofs)) || P.n != sys.n) {
+    if (!mf_analyse(P, dofs, s->g.Ny1, s->g.Nx1, mf_leaf(s, dofs)) || P.n != sys.n) {
         s->last_error = "multifrontal analysis failed";
         return EREBUS_EINVAL;
     }
@@ -948,7 +952,12 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
     if (e == cudaSuccess) e = upload(&D->eamap, P.eamap, s->stream);
     if (e == cudaSuccess) e = upload(&D->lvl, P.level_begin, s->stream);
     if (e == cudaSuccess) e = upload(&D->lvl_kt, lvl_kt, s->stream);
-    if (e == cudaSuccess) e = upload(&D->lvl_mode, mf_level_modes(P, mf_grid(s)), s->stream);
+    const int fops = s->opt.mf_local_factor_ops > 0 ? s->opt.mf_local_factor_ops
+                                                     : kLocalFactorOps;
+    const int stiles = s->opt.mf_local_solve_tiles > 0 ? s->opt.mf_local_solve_tiles
+                                                        : kLocalSolveTiles;
+    if (e == cudaSuccess)
+        e = upload(&D->lvl_mode, mf_level_modes(P, mf_grid(s), fops, stiles), s->stream);
     if (e == cudaSuccess) e = upload(&D->target, target, s->stream);
     if (e == cudaSuccess) e = upload(&D->expect, expect, s->stream);
     if (e == cudaSuccess) e = cudaMalloc(&D->vec, P.vec * sizeof(double));
@@ -1051,7 +1060,7 @@ int mf_convert_fp32(erebus_state *s, BandSystem &sys) {
 
 void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o) {
     MfPlan P;
-    mf_analyse(P, sys.dofs, s->g.Ny1, s->g.Nx1, mf_leaf(sys.dofs));
+    mf_analyse(P, sys.dofs, s->g.Ny1, s->g.Nx1, mf_leaf(s, sys.dofs));
     double tiles = 0.0, rd = 0.0;
     for (const MfFront &F : P.fronts) {
         tiles += F.Kt;   // inverses

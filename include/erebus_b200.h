@@ -202,6 +202,15 @@ typedef struct ErebusSolverOptions {
     int32_t precond_fp32;      /* 1: apply the preconditioner from FP32 factors */
     int32_t krylov_restart;    /* FGMRES restart length (1..64) */
     int32_t refactor_iterations; /* refresh the factors after a solve that took more */
+    /* Multifrontal analysis (no reference counterpart), 0 = the built-in
+       default; erebus_b200.autotune picks them per grid size by timing.
+       Changing them takes effect at the next analysis (a new state, or a
+       direct_solver / precision change). */
+    int32_t mf_leaf_vector;       /* nested-dissection leaf size, nodes, Stokes-Darcy (32) */
+    int32_t mf_leaf_scalar;       /* the same for the heat and gravity systems (64) */
+    int32_t mf_local_factor_ops;  /* a level factors one front per CTA when a CTA's
+                                     share is at most this many tile operations (8) */
+    int32_t mf_local_solve_tiles; /* ... and solves so when at most this many tiles (24) */
 } ErebusSolverOptions;
 
 /* Size and work of one system's direct solver (diagnostics; no reference

@@ -55,3 +55,29 @@ def test_run_simulation_writes_snapshots(pkg, built_lib, tmp_path):
     np.testing.assert_array_equal(ref.grid["tk1"], st.grid["tk1"])
     first = load_state(output_file(str(tmp_path), 2))
     assert first["timesum"] < last["timesum"]
+
+
+def test_snapshot_keeps_step_host_buffers(pkg, built_lib):
+    """Growing the snapshot staging leaves the buffers of erebus_step_host
+    alone: a run that snapshots between host timesteps ends bit for bit where
+    the run without the snapshot ends."""
+    a = pkg.make_state("planetesimal_41")
+    b = a.copy()
+    sa, sb = pkg.Simulation(a), pkg.Simulation(b)
+    sa.step_host(1)
+    sb.step_host(1)
+    sa.snapshot_begin(pkg.HostState(a.p, a.capacity, pinned=True))
+    sa.snapshot_wait()
+    for ts in (2, 3):
+        sa.step_host(ts)
+        sb.step_host(ts)
+    sa.close()
+    sb.close()
+    assert (a.marknum, a.dt, a.timesum) == (b.marknum, b.dt, b.timesum)
+    n = a.marknum
+    for k in a.m:
+        if k == "etasolidm_m":
+            continue
+        np.testing.assert_array_equal(a.m[k][:n], b.m[k][:n], err_msg=k)
+    for k in a.grid:
+        np.testing.assert_array_equal(a.grid[k], b.grid[k], err_msg=k)
