@@ -383,14 +383,22 @@ k_mf_factor(MfView V, unsigned int *bar, int *err) {
 // which a CTA keeps HBM reads in flight.
 constexpr int MF_SLOTS = 3;
 
+// A front of a one-front-per-CTA level whose vector has at most MF_VS_MAX
+// entries keeps it in shared memory for the whole sweep, so a tile costs
+// one CTA barrier and no round trip to L2.
+constexpr int MF_VS_MAX = 1024;
+
 struct MfSolveSmem {
     double tile[MF_SLOTS][T2];
     unsigned long long bar[MF_SLOTS];
-    double part[4][64];    // quarter partial sums
+    double part[2][4][64];  // quarter partial sums (two buffers, alternating tiles)
     double x[64];          // vector piece the current tile multiplies
     double y[64];
+    double vs[MF_VS_MAX];  // the front vector of a front swept by one CTA
     int2 km[MF_KM_MAX];    // (Kt, Mt) of the level's fronts
 };
+// two CTAs per SM
+static_assert(sizeof(MfSolveSmem) <= 113 * 1024, "solve shared memory");
 
 __device__ __forceinline__ uint32_t mf_smem(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -434,8 +442,10 @@ __device__ __forceinline__ void mf_slot_wait(MfSolveSmem &S, int sl, uint32_t pa
 
 // Streams the n tiles src(0..n-1) through the slots and calls use(i, tile)
 // with all threads once tile i is in shared memory.  uses[] counts the
-// phases of each slot's barrier (identical in every thread).
-template <class Src, class Use>
+// phases of each slot's barrier (identical in every thread).  With
+// `released`, use() itself ends every thread's reads of the tile before a
+// CTA barrier it passes, so the slot is refilled without another one.
+template <bool released = false, class Src, class Use>
 __device__ void mf_stream(MfSolveSmem &S, uint32_t *uses, int n, Src src, Use use, int *err) {
     for (int i = 0; i < n && i < MF_SLOTS; i++) mf_fetch(S, i, src(i));
     for (int i = 0; i < n; i++) {
@@ -443,7 +453,7 @@ __device__ void mf_stream(MfSolveSmem &S, uint32_t *uses, int n, Src src, Use us
         mf_slot_wait(S, sl, uses[sl] & 1u, err);
         uses[sl]++;
         use(i, (const decltype(src(0)))S.tile[sl]);
-        __syncthreads();
+        if (!released) __syncthreads();
         if (i + MF_SLOTS < n) mf_fetch(S, sl, src(i + MF_SLOTS));
     }
 }
@@ -467,14 +477,29 @@ __device__ __forceinline__ double mf_quarter(const T *Tt, const double *x) {
 // Reduces the quarter sums s of all threads: returns the row total in
 // threads 0..63 (row = tid).  Ends with a barrier.
 __device__ __forceinline__ double mf_reduce_rows(MfSolveSmem &S, double s) {
-    S.part[threadIdx.x >> 6][threadIdx.x & 63] = s;
+    S.part[0][threadIdx.x >> 6][threadIdx.x & 63] = s;
     __syncthreads();
     double t = 0.0;
     if (threadIdx.x < 64) {
         const int r = threadIdx.x;
-        t = (S.part[0][r] + S.part[1][r]) + (S.part[2][r] + S.part[3][r]);
+        t = (S.part[0][0][r] + S.part[0][1][r]) + (S.part[0][2][r] + S.part[0][3][r]);
     }
     __syncthreads();
+    return t;
+}
+
+// The same sum through buffer `b` with one barrier: consecutive calls
+// alternate the buffers, so a buffer is written again only after the
+// barrier of the call in between, when its readers (threads 0..63, right
+// after the barrier of their own call) are done with it.
+__device__ __forceinline__ double mf_reduce_rows1(MfSolveSmem &S, double s, int b) {
+    S.part[b][threadIdx.x >> 6][threadIdx.x & 63] = s;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x < 64) {
+        const int r = threadIdx.x;
+        t = (S.part[b][0][r] + S.part[b][1][r]) + (S.part[b][2][r] + S.part[b][3][r]);
+    }
     return t;
 }
 
@@ -613,6 +638,146 @@ __device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, doubl
             j++;
         },
         err);
+}
+
+// ---- one front per CTA, the front vector in shared memory ------------------
+// The same arithmetic as mf_gather_fwd + mf_fwd_front and mf_row_gemv +
+// mf_bwd_front, in the same order, for fronts with M <= MF_VS_MAX.
+
+// Forward sweep of front f: gather into S.vs, eliminate, write the vector
+// (pivot part for the backward sweep, update part for the parent) to V.vec.
+template <class T>
+__device__ void mf_fwd_front_s(const MfView &V, const MfFront &f, const double *w,
+                               MfSolveSmem &S, uint32_t *uses, int *err) {
+    double *vs = S.vs;
+    {
+        const int *var = V.vars + f.var_off, *map = V.eamap + f.map_off;
+        MfFront C0, C1;
+        const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
+        if (h0) C0 = V.fr[f.c0];
+        if (h1) C1 = V.fr[f.c1];
+        for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
+            int g = var[a];
+            double s = (a < f.Kp && g >= 0) ? __ldcg(&w[g]) : 0.0;
+            if (h0) {
+                int i = map[2 * a];
+                if (i >= 0) s += __ldcg(&V.vec[C0.vec_off + C0.Kp + i]);
+            }
+            if (h1) {
+                int i = map[2 * a + 1];
+                if (i >= 0) s += __ldcg(&V.vec[C1.vec_off + C1.Kp + i]);
+            }
+            vs[a] = s;
+        }
+    }
+    int n = 0;
+    for (int K = 0; K < f.Kt; K++) n += f.Mt - K - 1;
+    int K = 0, I = 1, b = 0;
+    int fk = 0, fi = 1;
+    auto src = [&](int) {
+        while (fi >= f.Mt) {
+            fk++;
+            fi = fk + 1;
+        }
+        const T *t = ftile<T>(V, f, fi, fk);
+        fi++;
+        return t;
+    };
+    __syncthreads();
+    mf_stream<true>(
+        S, uses, n, src,
+        [&](int, const T *Tt) {
+            while (I >= f.Mt) {
+                K++;
+                I = K + 1;
+            }
+            if (I == K + 1) __syncthreads();   // row K is final
+            double t = mf_reduce_rows1(S, mf_quarter(Tt, vs + K * 64), b);
+            b ^= 1;
+            if (threadIdx.x < 64) vs[I * 64 + threadIdx.x] -= t;
+            I++;
+        },
+        err);
+    __syncthreads();
+    double *v = V.vec + f.vec_off;
+    for (int a = threadIdx.x; a < f.M; a += blockDim.x) __stcg(&v[a], vs[a]);
+    __syncthreads();
+}
+
+// Backward sweep of front f: the ring solution (from w) and the pivot part
+// of the forward sweep into S.vs; rows K < Kt subtract the ring products
+// (all ring tiles streamed row after row), then the block substitution.
+// The solution goes to V.vec and to w.
+template <class T>
+__device__ void mf_bwd_front_s(const MfView &V, const MfFront &f, double *w, MfSolveSmem &S,
+                               uint32_t *uses, int *err) {
+    double *vs = S.vs, *v = V.vec + f.vec_off;
+    const int *var = V.vars + f.var_off;
+    for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
+        if (a < f.Kp) {
+            vs[a] = __ldcg(&v[a]);
+        } else {
+            int g = var[a];
+            vs[a] = g >= 0 ? __ldcg(&w[g]) : 0.0;
+        }
+    }
+    __syncthreads();
+    const int nr = f.Mt - f.Kt;
+    if (nr > 0) {
+        double acc = 0.0;
+        mf_stream(
+            S, uses, f.Kt * nr,
+            [&](int i) { return (const T *)ftile<T>(V, f, i / nr, f.Kt + i % nr); },
+            [&](int i, const T *Tt) {
+                acc += mf_quarter(Tt, vs + (f.Kt + i % nr) * 64);
+                if (i % nr == nr - 1) {
+                    double t = mf_reduce_rows(S, acc);
+                    if (threadIdx.x < 64) vs[(i / nr) * 64 + threadIdx.x] -= t;
+                    acc = 0.0;
+                }
+            },
+            err);
+    }
+    const int n = f.Kt * (f.Kt + 1) / 2;
+    int K = f.Kt - 1, j = 0, b = 0;
+    int fk = f.Kt - 1, fj = 0;
+    auto src = [&](int) {
+        if (fj > fk) {
+            fk--;
+            fj = 0;
+        }
+        const T *t = fj == 0 ? ftile<T>(V, f, fk, fk) : ftile<T>(V, f, fj - 1, fk);
+        fj++;
+        return t;
+    };
+    __syncthreads();
+    mf_stream<true>(
+        S, uses, n, src,
+        [&](int, const T *Tt) {
+            if (j > K) {
+                K--;
+                j = 0;
+            }
+            if (j == 0) {   // x_K = D_K^{-1} v_K
+                __syncthreads();   // row K is final
+                double x = mf_reduce_rows1(S, mf_quarter(Tt, vs + K * 64), b);
+                if (threadIdx.x < 64) {
+                    const int r = threadIdx.x, a = K * 64 + r;
+                    S.x[r] = x;
+                    vs[a] = x;
+                    __stcg(&v[a], x);
+                    if (a < f.k) __stcg(&w[var[a]], x);
+                }
+                __syncthreads();   // S.x is complete
+            } else {        // v_I -= U_IK x_K, I = j - 1
+                double t = mf_reduce_rows1(S, mf_quarter(Tt, S.x), b);
+                if (threadIdx.x < 64) vs[(j - 1) * 64 + threadIdx.x] -= t;
+            }
+            b ^= 1;
+            j++;
+        },
+        err);
+    __syncthreads();
 }
 
 // ---- cooperative levels: one task per 64-row block of a front --------------
@@ -772,6 +937,10 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
         if (local) {
             for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
                 const MfFront f = V.fr[fi];
+                if (f.M <= MF_VS_MAX) {
+                    mf_fwd_front_s<T>(V, f, w, S, uses, err);
+                    continue;
+                }
                 double *v = V.vec + f.vec_off;
                 mf_gather_fwd(V, f, w, v);
                 mf_fwd_front<T>(V, f, v, f.Mt, S, uses, err);
@@ -799,6 +968,10 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
         if (local) {
             for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
                 const MfFront f = V.fr[fi];
+                if (f.M <= MF_VS_MAX) {
+                    mf_bwd_front_s<T>(V, f, w, S, uses, err);
+                    continue;
+                }
                 double *v = V.vec + f.vec_off;
                 for (int K = 0; K < f.Kt && f.Mt > f.Kt; K++)
                     mf_row_gemv<T>(V, f, v, K, f.Kt, f.Mt, ring_x(f), S, uses, err);
