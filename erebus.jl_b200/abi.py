@@ -178,7 +178,7 @@ class ErebusSolverOptions(Structure):
         ("krylov", c_int32), ("precond_fp32", c_int32), ("krylov_restart", c_int32),
         ("refactor_iterations", c_int32), ("mf_leaf_vector", c_int32),
         ("mf_leaf_scalar", c_int32), ("mf_local_factor_ops", c_int32),
-        ("mf_local_solve_tiles", c_int32),
+        ("mf_local_solve_tiles", c_int32), ("mf_block_substitution", c_int32),
     ]
 
 

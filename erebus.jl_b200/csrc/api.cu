@@ -225,6 +225,7 @@ int erebus_default_solver_options(ErebusSolverOptions *o) {
     o->mf_leaf_scalar = 0;
     o->mf_local_factor_ops = 0;
     o->mf_local_solve_tiles = 0;
+    o->mf_block_substitution = 0;
     return EREBUS_OK;
 }
 
@@ -424,7 +425,8 @@ int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o) {
     if (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL && o->direct_solver != EREBUS_SOLVER_BAND)
         return EREBUS_EINVAL;
     if (o->mf_leaf_vector < 0 || o->mf_leaf_scalar < 0 || o->mf_local_factor_ops < 0 ||
-        o->mf_local_solve_tiles < 0)
+        o->mf_local_solve_tiles < 0 ||
+        (o->mf_block_substitution != 0 && o->mf_block_substitution != 1))
         return EREBUS_EINVAL;
     if (o->krylov && (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL || o->factor_fp32 ||
                       o->krylov_restart < 1 || o->krylov_restart > KRYLOV_MAX_RESTART ||
@@ -433,7 +435,8 @@ int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o) {
     if (o->mf_leaf_vector != s->opt.mf_leaf_vector ||
         o->mf_leaf_scalar != s->opt.mf_leaf_scalar ||
         o->mf_local_factor_ops != s->opt.mf_local_factor_ops ||
-        o->mf_local_solve_tiles != s->opt.mf_local_solve_tiles) {   // analysed again
+        o->mf_local_solve_tiles != s->opt.mf_local_solve_tiles ||
+        o->mf_block_substitution != s->opt.mf_block_substitution) {   // analysed again
         for (BandSystem *b : {&s->hydro, &s->thermal, &s->gravity}) {
             mf_release(*b);
             b->factored = false;

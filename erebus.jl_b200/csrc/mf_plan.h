@@ -40,6 +40,7 @@ struct MfFront {
     int Kt, Mt;          // Kp / 64, M / 64
     int parent, c0, c1;  // front indices (-1: none)
     int level;           // depth in the tree (root 0)
+    long long poff;      // offset of the solve's partial sums (-1: none; set by the solver)
 };
 
 struct MfPlan {
@@ -178,6 +179,7 @@ inline bool mf_analyse(MfPlan &P, int d, int ny, int nx, int leaf) {
         F.Kt = F.Kp / MF_TILE;
         F.Mt = F.M / MF_TILE;
         F.level = nd.depth;
+        F.poff = -1;
         F.off = off;
         F.var_off = voff;
         F.map_off = 2 * voff;

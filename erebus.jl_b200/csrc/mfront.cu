@@ -48,6 +48,9 @@ struct MfView {
     const int *lvl_kt;  // max Kt per level
     const int *lvl_mode;  // per level: MF_FACTOR_LOCAL, MF_SOLVE_LOCAL bits
     int *flags;         // per 64-row block of the front vectors: the solve epoch it is final in
+    double *vec2;       // pivot part of the forward solution (levels with inverted pivot blocks)
+    double *part;       // partial sums of the backward ring products (MfFront::poff)
+    int inv;            // cooperative solve levels hold inverted pivot blocks
     int nlev;
     const long long *target;   // ELL entry -> storage offset
     const int *expect;         // ELL column pattern the targets were built from
@@ -66,6 +69,11 @@ struct MfDevice {
     int *lvl_mode = nullptr;
     int *flags = nullptr;   // row-block flags of the cooperative solve levels
     int epoch = 0;          // solves launched so far
+    // inverted pivot blocks of the cooperative solve levels
+    bool inv = false;
+    double *vec2 = nullptr, *part = nullptr;
+    int2 *inv_list = nullptr;   // (front, Kt) of the fronts k_mf_invert works on
+    int n_inv = 0, inv_ktmax = 0;
     long long *target = nullptr;
     int *expect = nullptr;
     int nlev = 0;
@@ -371,6 +379,116 @@ k_mf_factor(MfView V, unsigned int *bar, int *err) {
                 mf_update_tile<T>(V, f, f.Kt + u % ru, f.Kt + u / ru, 0, f.Kt, S, err, false);
             });
         grid_barrier(bar, err);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// inverted pivot blocks (fronts of the cooperative solve levels)
+// ---------------------------------------------------------------------------
+// After the factorisation, the pivot block of a front holds the block-unit-
+// lower L (tiles (I,K), I > K), the diagonal inverses D_K^{-1} (tiles (K,K))
+// and the block-upper U's off-diagonal tiles (K,J), K < J.  k_mf_invert
+// replaces them in place by
+//   Y = I - L^{-1}                      below the diagonal,
+//   Z_KJ = -(U^{-1})_KJ = Y'_KJ D_J^{-1}  above it (Y' = I - (I + D^{-1} N)^{-1},
+//                                         N the strictly upper part of U),
+// keeping D_K^{-1} on the diagonal, so that the triangular solves of the
+// pivot block become products whose row blocks are independent:
+//   y = v_P - Y v_P,   x_K = D_K^{-1} t_K - sum_{J > K} Z_KJ t_J.
+// Right-looking, in place, on the tile products of the factorisation:
+//   step 0:           U~_KJ = D_K^{-1} U_KJ                 (K < J)
+//   step s, 1..Kt-2:  Y_IK  -= L_Is Y_sK   (I > s > K)
+//                     Y'_KJ -= Y'_Ks U~_sJ (K < s < J)
+//   step Kt-1:        Z_KJ = Y'_KJ D_J^{-1}                 (K < J)
+// Step s reads row and column s only and writes neither, and a tile's last
+// update comes before the step that reads it.
+
+// the (K, J), K < J, of triangular index u (column J holds J entries)
+__device__ __forceinline__ void mf_tri(int u, int &K, int &J) {
+    J = 1;
+    while ((J + 1) * J / 2 <= u) J++;
+    K = u - J * (J - 1) / 2;
+}
+
+__device__ __forceinline__ int mf_inv_count(int s, int Kt) {
+    if (Kt < 2) return 0;
+    if (s == 0 || s == Kt - 1) return Kt * (Kt - 1) / 2;
+    if (s < Kt - 1) return 2 * s * (Kt - 1 - s);
+    return 0;
+}
+
+// tile C = tile A * tile B (C may be A or B)
+template <class T>
+__device__ void mf_tile_mul(T *C, const T *At, const T *Bt, MmaSmem &S) {
+    typename MfAccT<T>::type acc;
+    typedef typename std::remove_reference<decltype(acc[0][0][0])>::type A;
+    mma_tiles(
+        S, 1, [&](int) { return At; }, [&](int) { return Bt; }, acc, [&] { frag_zero(acc); });
+    frag_store(C, acc, A(1));
+    __syncthreads();
+}
+
+// tile C -= tile A * tile B
+template <class T>
+__device__ void mf_tile_sub_mul(T *C, const T *At, const T *Bt, MmaSmem &S) {
+    typename MfAccT<T>::type acc;
+    typedef typename std::remove_reference<decltype(acc[0][0][0])>::type A;
+    mma_tiles(
+        S, 1, [&](int) { return At; }, [&](int) { return Bt; }, acc,
+        [&] { frag_load(C, acc, A(-1)); });
+    frag_store(C, acc, A(-1));
+    __syncthreads();
+}
+
+template <class T>
+__device__ void mf_inv_task(const MfView &V, const MfFront &f, int s, int u, MmaSmem &S) {
+    const int Kt = f.Kt;
+    auto t = [&](int I, int J) { return ftile<T>(V, f, I, J); };
+    int I, J, K;
+    if (s == 0) {
+        mf_tri(u, K, J);
+        mf_tile_mul<T>(t(K, J), t(K, K), t(K, J), S);
+    } else if (s == Kt - 1) {
+        mf_tri(u, K, J);
+        mf_tile_mul<T>(t(K, J), t(K, J), t(J, J), S);
+    } else {
+        const int e = Kt - 1 - s;
+        if (u < s * e) {
+            I = s + 1 + u % e;
+            K = u / e;
+            mf_tile_sub_mul<T>(t(I, K), t(I, s), t(s, K), S);
+        } else {
+            u -= s * e;
+            K = u % s;
+            J = s + 1 + u / s;
+            mf_tile_sub_mul<T>(t(K, J), t(K, s), t(s, J), S);
+        }
+    }
+}
+
+// All listed fronts at once: step s of every front, then a grid barrier.
+// Tasks are numbered across the fronts and dealt round-robin, as in
+// mf_for_tasks.
+template <class T>
+__global__ void __launch_bounds__(LU_THREADS, 2)
+k_mf_invert(MfView V, const int2 *list, int nlist, int ktmax, unsigned int *bar, int *err) {
+    extern __shared__ __align__(16) double smem_raw[];
+    MfFactorSmem &FS = *reinterpret_cast<MfFactorSmem *>(smem_raw);
+    const int G = gridDim.x;
+    for (int s = 0; s < ktmax; s++) {
+        int first = blockIdx.x;
+        for (int q = 0; q < nlist; q++) {
+            const int2 e = list[q];
+            const int cnt = mf_inv_count(s, e.y);
+            if (cnt <= 0) continue;
+            if (first < cnt) {
+                const MfFront f = V.fr[e.x];
+                for (int u = first; u < cnt; u += G) mf_inv_task<T>(V, f, s, u, FS.m);
+            }
+            first -= cnt;
+            if (first < 0) first = first % G + (first % G < 0 ? G : 0);
+        }
+        if (s + 1 < ktmax) grid_barrier(bar, err);
     }
 }
 
@@ -912,6 +1030,134 @@ __device__ void mf_bwd_row(const MfView &V, const MfFront &f, double *w, int K, 
     __syncthreads();
 }
 
+// ---- cooperative levels with inverted pivot blocks -------------------------
+// Per level, forward: (F1) pivot rows y_I = v_I - sum_{K<I} Y_IK v_K into
+// vec2, (F2) update rows v_I -= sum_{K<Kt} L_IK y_K; backward: (B1) partial
+// ring products sum_{J in chunk} U_KJ x_J of the pivot rows, (B2)
+// x_K = D_K^{-1} t_K - sum_{J>K} Z_KJ t_J with t_J = y_J minus its partials.
+// v is gathered where it is read (children's update parts and the right-
+// hand side), so each sweep of a level takes two phases, and every task is
+// one row block: no task waits for another inside a phase.
+constexpr int MF_XG = MF_VS_MAX / 64;    // vector pieces staged in shared memory at a time
+constexpr int MF_RING_CHUNK = MF_XG;      // ring tiles per backward partial sum
+static_assert(MF_XG * 64 == 4 * LU_THREADS, "staging: four elements per thread");
+
+__host__ __device__ __forceinline__ int mf_ring_chunks(int nr) {
+    return (nr + MF_RING_CHUNK - 1) / MF_RING_CHUNK;
+}
+
+// Per-thread quarter sums of sum_{i<n} sign(i) T_i x_i: tile(i) points to
+// T_i, piece(i, c) gives element c of x_i; the pieces are staged in
+// S.vs MF_XG at a time while the tiles stream.
+template <class T, class Tile, class Piece, class Sign>
+__device__ double mf_row_tiles(MfSolveSmem &S, uint32_t *uses, int n, Tile tile, Piece piece,
+                               Sign sign, int *err) {
+    double acc = 0.0;
+    mf_stream(
+        S, uses, n, tile,
+        [&](int i, const T *Tt) {
+            if (i % MF_XG == 0) {   // the previous tile's barrier has passed
+                const int m = min(n - i, MF_XG) * 64;
+                double v[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int e = threadIdx.x + q * LU_THREADS;
+                    v[q] = e < m ? piece(i + (e >> 6), e & 63) : 0.0;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int e = threadIdx.x + q * LU_THREADS;
+                    if (e < m) S.vs[e] = v[q];
+                }
+                __syncthreads();
+            }
+            acc += sign(i) * mf_quarter(Tt, S.vs + (i % MF_XG) * 64);
+        },
+        err);
+    return acc;
+}
+
+// F1: pivot row block I of front f.
+template <class T>
+__device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, int I,
+                          MfSolveSmem &S, uint32_t *uses, int *err) {
+    const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
+    MfFront C0, C1;
+    if (h0) C0 = V.fr[f.c0];
+    if (h1) C1 = V.fr[f.c1];
+    double g = 0.0;
+    if (threadIdx.x < 64) g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
+    const double acc = mf_row_tiles<T>(
+        S, uses, I, [&](int K) { return (const T *)ftile<T>(V, f, I, K); },
+        [&](int K, int c) { return mf_gather_elem(V, f, w, K * 64 + c, h0, C0, h1, C1); },
+        [](int) { return 1.0; }, err);
+    const double t = mf_reduce_rows(S, acc);
+    if (threadIdx.x < 64) __stcg(&V.vec2[f.vec_off + I * 64 + threadIdx.x], g - t);
+}
+
+// F2: update row block I (>= Kt) of front f.
+template <class T>
+__device__ void mf_inv_f2(const MfView &V, const MfFront &f, const double *w, int I,
+                          MfSolveSmem &S, uint32_t *uses, int *err) {
+    const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
+    MfFront C0, C1;
+    if (h0) C0 = V.fr[f.c0];
+    if (h1) C1 = V.fr[f.c1];
+    double g = 0.0;
+    if (threadIdx.x < 64) g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
+    const double *y = V.vec2 + f.vec_off;
+    const double acc = mf_row_tiles<T>(
+        S, uses, f.Kt, [&](int K) { return (const T *)ftile<T>(V, f, I, K); },
+        [&](int K, int c) { return __ldcg(&y[K * 64 + c]); }, [](int) { return 1.0; }, err);
+    const double t = mf_reduce_rows(S, acc);
+    if (threadIdx.x < 64) __stcg(&V.vec[f.vec_off + I * 64 + threadIdx.x], g - t);
+}
+
+// B1: ring tiles [Kt + 16 ch, ...) of pivot row block K of front f.
+template <class T>
+__device__ void mf_inv_b1(const MfView &V, const MfFront &f, const double *w, int K, int ch,
+                          MfSolveSmem &S, uint32_t *uses, int *err) {
+    const int nr = f.Mt - f.Kt, nch = mf_ring_chunks(nr), j0 = f.Kt + ch * MF_RING_CHUNK;
+    const int n = min(MF_RING_CHUNK, f.Mt - j0);
+    const int *var = V.vars + f.var_off;
+    const double acc = mf_row_tiles<T>(
+        S, uses, n, [&](int j) { return (const T *)ftile<T>(V, f, K, j0 + j); },
+        [&](int j, int c) {
+            const int g = var[(j0 + j) * 64 + c];
+            return g >= 0 ? __ldcg(&w[g]) : 0.0;
+        },
+        [](int) { return 1.0; }, err);
+    const double t = mf_reduce_rows(S, acc);
+    if (threadIdx.x < 64)
+        __stcg(&V.part[f.poff + ((long long)K * nch + ch) * 64 + threadIdx.x], t);
+}
+
+// B2: pivot row block K of front f; the solution goes to w.
+template <class T>
+__device__ void mf_inv_b2(const MfView &V, const MfFront &f, double *w, int K, MfSolveSmem &S,
+                          uint32_t *uses, int *err) {
+    const int nch = mf_ring_chunks(f.Mt - f.Kt);
+    const double *y = V.vec2 + f.vec_off;
+    const int *var = V.vars + f.var_off;
+    const double acc = mf_row_tiles<T>(
+        S, uses, f.Kt - K, [&](int i) { return (const T *)ftile<T>(V, f, K, K + i); },
+        [&](int i, int c) {
+            const int J = K + i;
+            double t = __ldcg(&y[J * 64 + c]);
+            if (nch > 0) {
+                const double *pp = V.part + f.poff + (long long)J * nch * 64 + c;
+                for (int ch = 0; ch < nch; ch++) t -= __ldcg(&pp[ch * 64]);
+            }
+            return t;
+        },
+        [](int i) { return i == 0 ? 1.0 : -1.0; }, err);
+    const double x = mf_reduce_rows(S, acc);
+    if (threadIdx.x < 64) {
+        const int a = K * 64 + threadIdx.x;
+        if (a < f.k) __stcg(&w[var[a]], x);
+    }
+}
+
 // Solves L U x = w in place (w: n values; rows >= n untouched).
 template <class T>
 __global__ void __launch_bounds__(LU_THREADS, 2)
@@ -945,6 +1191,14 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
                 mf_gather_fwd(V, f, w, v);
                 mf_fwd_front<T>(V, f, v, f.Mt, S, uses, err);
             }
+        } else if (V.inv) {
+            mf_for_tasks(
+                V, fb, fe, S.km, [](int Kt, int) { return Kt; },
+                [&](const MfFront &f, int I) { mf_inv_f1<T>(V, f, w, I, S, uses, err); });
+            grid_barrier(bar, err);
+            mf_for_tasks(
+                V, fb, fe, S.km, [](int Kt, int Mt) { return Mt - Kt; },
+                [&](const MfFront &f, int u) { mf_inv_f2<T>(V, f, w, f.Kt + u, S, uses, err); });
         } else {
             // one task per row block, in increasing order within each front
             mf_for_tasks(
@@ -977,6 +1231,17 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
                     mf_row_gemv<T>(V, f, v, K, f.Kt, f.Mt, ring_x(f), S, uses, err);
                 mf_bwd_front<T>(V, f, v, w, S, uses, err);
             }
+        } else if (V.inv) {
+            mf_for_tasks(
+                V, fb, fe, S.km, [](int Kt, int Mt) { return Kt * mf_ring_chunks(Mt - Kt); },
+                [&](const MfFront &f, int u) {
+                    const int nch = mf_ring_chunks(f.Mt - f.Kt);
+                    mf_inv_b1<T>(V, f, w, u / nch, u % nch, S, uses, err);
+                });
+            grid_barrier(bar, err);
+            mf_for_tasks(
+                V, fb, fe, S.km, [](int Kt, int) { return Kt; },
+                [&](const MfFront &f, int K) { mf_inv_b2<T>(V, f, w, K, S, uses, err); });
         } else {
             // one task per pivot row block, the last first
             mf_for_tasks(
@@ -1003,6 +1268,9 @@ static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
     V.lvl_kt = D.lvl_kt;
     V.lvl_mode = D.lvl_mode;
     V.flags = D.flags;
+    V.vec2 = D.vec2;
+    V.part = D.part;
+    V.inv = D.inv ? 1 : 0;
     V.nlev = D.nlev;
     V.target = D.target;
     V.expect = D.expect;
@@ -1017,7 +1285,7 @@ void mf_release(BandSystem &sys) {
     MfDevice *D = sys.mf;
     if (!D) return;
     void *ps[] = {D->fr, D->F64, D->F32, D->vec, D->vars, D->eamap, D->lvl, D->lvl_kt,
-                  D->lvl_mode, D->flags, D->target, D->expect};
+                  D->lvl_mode, D->flags, D->target, D->expect, D->vec2, D->part, D->inv_list};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete D;
@@ -1034,7 +1302,7 @@ static cudaError_t upload(T **dst, const std::vector<T> &src, cudaStream_t st) {
 }
 
 // CTAs of the cooperative factor and solve launches (2 per SM).
-static int mf_grid(erebus_state *s) {
+static int mf_grid(const erebus_state *s) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
     return 2 * sms;
@@ -1120,17 +1388,41 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
         lvl_kt.push_back(m);
     }
     D->nlev = (int)P.level_begin.size() - 1;
+    const int fops = s->opt.mf_local_factor_ops > 0 ? s->opt.mf_local_factor_ops
+                                                     : kLocalFactorOps;
+    const int stiles = s->opt.mf_local_solve_tiles > 0 ? s->opt.mf_local_solve_tiles
+                                                        : kLocalSolveTiles;
+    const std::vector<int> modes = mf_level_modes(P, mf_grid(s), fops, stiles);
+    // cooperative solve levels: inverted pivot blocks, partial-sum storage
+    D->inv = s->opt.mf_block_substitution == 0;
+    std::vector<int2> inv;
+    long long poff = 0;
+    for (int p = 0; D->inv && p < D->nlev; p++) {
+        if (modes[p] & MF_SOLVE_LOCAL) continue;
+        for (int fi = P.level_begin[p]; fi < P.level_begin[p + 1]; fi++) {
+            MfFront &F = P.fronts[fi];
+            const int nch = mf_ring_chunks(F.Mt - F.Kt);
+            if (nch > 0 && F.Kt > 0) {
+                F.poff = poff;
+                poff += (long long)F.Kt * nch * 64;
+            }
+            if (F.Kt >= 2) {
+                inv.push_back(make_int2(fi, F.Kt));
+                D->inv_ktmax = std::max(D->inv_ktmax, F.Kt);
+            }
+        }
+    }
+    D->n_inv = (int)inv.size();
     cudaError_t e = upload(&D->fr, P.fronts, s->stream);
     if (e == cudaSuccess) e = upload(&D->vars, P.vars, s->stream);
     if (e == cudaSuccess) e = upload(&D->eamap, P.eamap, s->stream);
     if (e == cudaSuccess) e = upload(&D->lvl, P.level_begin, s->stream);
     if (e == cudaSuccess) e = upload(&D->lvl_kt, lvl_kt, s->stream);
-    const int fops = s->opt.mf_local_factor_ops > 0 ? s->opt.mf_local_factor_ops
-                                                     : kLocalFactorOps;
-    const int stiles = s->opt.mf_local_solve_tiles > 0 ? s->opt.mf_local_solve_tiles
-                                                        : kLocalSolveTiles;
-    if (e == cudaSuccess)
-        e = upload(&D->lvl_mode, mf_level_modes(P, mf_grid(s), fops, stiles), s->stream);
+    if (e == cudaSuccess) e = upload(&D->lvl_mode, modes, s->stream);
+    if (e == cudaSuccess && D->inv) e = upload(&D->inv_list, inv, s->stream);
+    if (e == cudaSuccess && D->inv) e = cudaMalloc(&D->vec2, P.vec * sizeof(double));
+    if (e == cudaSuccess && D->inv)
+        e = cudaMalloc(&D->part, std::max<long long>(poff, 1) * sizeof(double));
     if (e == cudaSuccess) e = upload(&D->target, target, s->stream);
     if (e == cudaSuccess) e = upload(&D->expect, expect, s->stream);
     if (e == cudaSuccess) e = cudaMalloc(&D->vec, P.vec * sizeof(double));
@@ -1187,6 +1479,20 @@ static int mf_factor_t(erebus_state *s, BandSystem &sys) {
     cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
     rc = coop_launch(s, fn, blocks, LU_THREADS, args, smem, "mf_factor launch");
     s->launches++;
+    if (rc || !D.inv || D.n_inv == 0) return rc;
+    const void *fi = (const void *)k_mf_invert<T>;
+    cudaFuncSetAttribute(fi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    blocks = mf_blocks(s, fi, smem);
+    if (blocks < 1) {
+        s->last_error = "mf_invert: kernel does not fit";
+        return EREBUS_ECUDA;
+    }
+    const int2 *list = D.inv_list;
+    int nlist = D.n_inv, ktmax = D.inv_ktmax;
+    void *iargs[] = {&V, &list, &nlist, &ktmax, &bar, &err};
+    cudaMemsetAsync(sys.bar, 0, 4 * sizeof(unsigned int), s->stream);
+    rc = coop_launch(s, fi, blocks, LU_THREADS, iargs, smem, "mf_invert launch");
+    s->launches++;
     return rc;
 }
 
@@ -1235,6 +1541,20 @@ void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o
     MfPlan P;
     mf_analyse(P, sys.dofs, s->g.Ny1, s->g.Nx1, mf_leaf(s, sys.dofs));
     double tiles = 0.0, rd = 0.0;
+    if (s->opt.mf_block_substitution == 0) {   // inversion of the cooperative levels' pivot blocks
+        const int fops = s->opt.mf_local_factor_ops > 0 ? s->opt.mf_local_factor_ops
+                                                         : kLocalFactorOps;
+        const int stiles = s->opt.mf_local_solve_tiles > 0 ? s->opt.mf_local_solve_tiles
+                                                            : kLocalSolveTiles;
+        const std::vector<int> modes = mf_level_modes(P, mf_grid(s), fops, stiles);
+        for (size_t p = 0; p < modes.size(); p++) {
+            if (modes[p] & MF_SOLVE_LOCAL) continue;
+            for (int fi = P.level_begin[p]; fi < P.level_begin[p + 1]; fi++) {
+                const double kt = P.fronts[fi].Kt;
+                if (kt >= 2) tiles += kt * (kt - 1) + (kt - 2) * (kt - 1) * kt / 3.0;
+            }
+        }
+    }
     for (const MfFront &F : P.fronts) {
         tiles += F.Kt;   // inverses
         for (int K = 0; K < F.Kt; K++) {

@@ -311,6 +311,7 @@ struct ErebusSolverOptions
     mf_leaf_scalar::Cint
     mf_local_factor_ops::Cint
     mf_local_solve_tiles::Cint
+    mf_block_substitution::Cint
 end
 
 const MARKER_FIELDS = (:xm, :ym, :tm, :tkm, :sxxm, :sxym, :etavpm, :phim, :phinewm, :pfm0, :XWsolidm, :XWsolidm0, :rhototalm, :rhocptotalm, :etatotalm, :hrtotalm, :ktotalm, :tkm_rhocptotalm, :etafluidcur_inv_kphim, :inv_gggtotalm, :fricttotalm, :cohestotalm, :tenstotalm, :rhofluidcur, :alphasolidcur, :alphafluidcur, :etasolidm_m)

@@ -45,6 +45,105 @@ bool invert(double *A) {   // Gauss-Jordan, no pivoting, in place
     }
     return true;
 }
+// The pivot-block inversion of the device solver's cooperative levels
+// (k_mf_invert, mfront.cu), step by step with the same task numbering:
+// tiles below the diagonal become Y = I - L^{-1}, above it
+// Z_KJ = Y'_KJ D_J^{-1} with Y' = I - (I + D^{-1} N)^{-1}.
+void invert_pivots(std::vector<double> &S, const MfFront &F) {
+    const int Kt = F.Kt;
+    if (Kt < 2) return;
+    std::vector<double> tmp(T * T);
+    auto t = [&](int I, int J) { return tile(S, F, I, J); };
+    auto mul = [&](double *C, const double *A, const double *B) {
+        std::fill(tmp.begin(), tmp.end(), 0.0);
+        gemm(tmp.data(), A, B, 1.0);
+        std::memcpy(C, tmp.data(), sizeof(double) * T * T);
+    };
+    for (int s = 0; s < Kt; s++) {
+        const int cnt = (s == 0 || s == Kt - 1) ? Kt * (Kt - 1) / 2 : 2 * s * (Kt - 1 - s);
+        for (int u = 0; u < cnt; u++) {
+            if (s == 0 || s == Kt - 1) {
+                int J = 1;
+                while ((J + 1) * J / 2 <= u) J++;
+                const int K = u - J * (J - 1) / 2;
+                if (s == 0) mul(t(K, J), t(K, K), t(K, J));
+                else mul(t(K, J), t(K, J), t(J, J));
+            } else {
+                const int e = Kt - 1 - s;
+                if (u < s * e) gemm(t(s + 1 + u % e, u / e), t(s + 1 + u % e, s), t(s, u / e), -1.0);
+                else {
+                    const int v = u - s * e, K = v % s, J = s + 1 + v / s;
+                    gemm(t(K, J), t(K, s), t(s, J), -1.0);
+                }
+            }
+        }
+    }
+}
+int solve_inverted(const MfPlan &P, std::vector<double> &S, const double *b, double *x) {
+    std::vector<double> w(b, b + P.n), fv(P.vec, 0.0), fy(P.vec, 0.0);
+    for (size_t f = 0; f < P.fronts.size(); f++) {
+        const MfFront &F = P.fronts[f];
+        double *v = &fv[F.vec_off], *y = &fy[F.vec_off];
+        const int *var = &P.vars[F.var_off];
+        const int *m = &P.eamap[F.map_off];
+        for (int a = 0; a < F.M; a++) {
+            double s = (a < F.Kp && var[a] >= 0) ? w[var[a]] : 0.0;
+            for (int q = 0; q < 2; q++) {
+                int c = q == 0 ? F.c0 : F.c1;
+                if (c >= 0 && m[2 * a + q] >= 0) s += fv[P.fronts[c].vec_off + P.fronts[c].Kp + m[2 * a + q]];
+            }
+            v[a] = s;
+        }
+        for (int I = 0; I < F.Kt; I++) {          // y_I = v_I - sum_K Y_IK v_K
+            for (int r = 0; r < T; r++) y[I * T + r] = v[I * T + r];
+            for (int K = 0; K < I; K++) {
+                const double *Y = tile(S, F, I, K);
+                for (int c = 0; c < T; c++)
+                    for (int r = 0; r < T; r++) y[I * T + r] -= Y[c * T + r] * v[K * T + c];
+            }
+        }
+        for (int I = F.Kt; I < F.Mt; I++)         // update rows
+            for (int K = 0; K < F.Kt; K++) {
+                const double *L = tile(S, F, I, K);
+                for (int c = 0; c < T; c++)
+                    for (int r = 0; r < T; r++) v[I * T + r] -= L[c * T + r] * y[K * T + c];
+            }
+    }
+    for (size_t f = P.fronts.size(); f-- > 0;) {
+        const MfFront &F = P.fronts[f];
+        double *v = &fv[F.vec_off], *y = &fy[F.vec_off];
+        const int *var = &P.vars[F.var_off];
+        for (int a = F.Kp; a < F.M; a++) v[a] = var[a] >= 0 ? w[var[a]] : 0.0;
+        std::vector<double> t(F.Kp);
+        for (int K = 0; K < F.Kt; K++) {          // t_K = y_K - ring partials, 16 tiles each
+            for (int r = 0; r < T; r++) t[K * T + r] = y[K * T + r];
+            for (int j0 = F.Kt; j0 < F.Mt; j0 += 16) {
+                double p[T] = {0.0};
+                for (int J = j0; J < std::min(F.Mt, j0 + 16); J++) {
+                    const double *U = tile(S, F, K, J);
+                    for (int c = 0; c < T; c++)
+                        for (int r = 0; r < T; r++) p[r] += U[c * T + r] * v[J * T + c];
+                }
+                for (int r = 0; r < T; r++) t[K * T + r] -= p[r];
+            }
+        }
+        for (int K = 0; K < F.Kt; K++) {          // x_K = D_K^{-1} t_K - sum_J Z_KJ t_J
+            const double *Di = tile(S, F, K, K);
+            for (int r = 0; r < T; r++) {
+                double s = 0.0;
+                for (int c = 0; c < T; c++) s += Di[c * T + r] * t[K * T + c];
+                for (int J = K + 1; J < F.Kt; J++) {
+                    const double *Z = tile(S, F, K, J);
+                    for (int c = 0; c < T; c++) s -= Z[c * T + r] * t[J * T + c];
+                }
+                v[K * T + r] = s;
+            }
+        }
+        for (int a = 0; a < F.k; a++) w[var[a]] = v[a];
+    }
+    std::memcpy(x, w.data(), sizeof(double) * P.n);
+    return 0;
+}
 }  // namespace
 
 extern "C" {
@@ -64,8 +163,12 @@ int mf_check_stats(int d, int ny, int nx, int leaf, long long *out) {
 // Solves the ELL system (rows x ell, rows >= n; rows >= n are ignored) for
 // right-hand side b (n values) into x.  Returns 0, or 1 analysis failed,
 // 2 entry outside the fronts, 3 zero pivot.
+// With `inverted`, every front's pivot block is inverted after its
+// factorisation and the sweeps take the device's inverted form: y_P = v_P -
+// Y v_P, ring products in partial sums of 16 tiles, x_K = D_K^{-1} t_K -
+// sum_{J>K} Z_KJ t_J.
 int mf_check_solve(int d, int ny, int nx, int leaf, const int *cols, const double *vals,
-                   long long rows, int ell, const double *b, double *x) {
+                   long long rows, int ell, const double *b, double *x, int inverted) {
     MfPlan P;
     if (!mf_analyse(P, d, ny, nx, leaf)) return 1;
     std::vector<long long> target;
@@ -108,6 +211,10 @@ int mf_check_solve(int d, int ny, int nx, int leaf, const int *cols, const doubl
             for (int I = F.Kt; I < F.Mt; I++)
                 for (int K = 0; K < F.Kt; K++)
                     gemm(tile(S, F, I, J), tile(S, F, I, K), tile(S, F, K, J), -1.0);
+    }
+    if (inverted) {
+        for (const MfFront &F : P.fronts) invert_pivots(S, F);
+        return solve_inverted(P, S, b, x);
     }
     // forward sweep
     std::vector<double> w(b, b + P.n), fv(P.vec, 0.0);

@@ -29,7 +29,7 @@ def mf(tmp_path_factory):
     L = ctypes.CDLL(so)
     P = ctypes.c_void_p
     L.mf_check_solve.argtypes = [ctypes.c_int] * 4 + [P, P, ctypes.c_longlong, ctypes.c_int,
-                                                      P, P]
+                                                      P, P, ctypes.c_int]
     L.mf_check_stats.argtypes = [ctypes.c_int] * 4 + [P]
     return L
 
@@ -56,11 +56,12 @@ def _ell(A):
     return As, cols, vals, 1.0 / rs, ell
 
 
-def _solve(mf, d, ny, nx, leaf, A, b):
+def _solve(mf, d, ny, nx, leaf, A, b, inverted=0):
     As, cols, vals, sc, ell = _ell(A)
     bs = b * sc
     x = np.zeros(A.shape[0])
-    rc = mf.mf_check_solve(d, ny, nx, leaf, _a(cols), _a(vals), A.shape[0], ell, _a(bs), _a(x))
+    rc = mf.mf_check_solve(d, ny, nx, leaf, _a(cols), _a(vals), A.shape[0], ell, _a(bs), _a(x),
+                           inverted)
     assert rc == 0, rc
     res = np.linalg.norm(bs - As @ x) / np.linalg.norm(bs)
     return x, res, As, bs
@@ -79,11 +80,15 @@ def stepped(pkg, oracle):
 
 
 @pytest.mark.parametrize("leaf", [4, 16, 32, 64])
-def test_hydromech_matches_superlu(mf, stepped, leaf):
+@pytest.mark.parametrize("inverted", [0, 1])
+def test_hydromech_matches_superlu(mf, stepped, leaf, inverted):
+    """Both forms of the sweeps: block substitution, and the inverted pivot
+    blocks of the device's cooperative levels (here on every front; the top
+    fronts at 41 x 41 have four 64-wide pivot blocks)."""
     st, o = stepped
     A, b = o.hydromech_system(st.dt)
     g = st.g
-    x, res, As, bs = _solve(mf, 6, g.Ny1, g.Nx1, leaf, A, b)
+    x, res, As, bs = _solve(mf, 6, g.Ny1, g.Nx1, leaf, A, b, inverted)
     ref = spla.splu(sp.csc_matrix(As)).solve(bs)
     assert res < 1e-9, res
     for t in range(6):
@@ -103,8 +108,9 @@ def test_thermal_and_gravity(mf, stepped):
 
 
 @pytest.mark.parametrize("ny,nx,d,leaf", [(9, 13, 2, 4), (20, 7, 3, 6), (1, 30, 1, 4),
-                                          (33, 33, 1, 1)])
-def test_rectangles_random(mf, ny, nx, d, leaf):
+                                          (33, 33, 1, 1), (40, 44, 6, 16)])
+@pytest.mark.parametrize("inverted", [0, 1])
+def test_rectangles_random(mf, ny, nx, d, leaf, inverted):
     """Rectangular grids and other block sizes: a random diagonally dominant
     matrix with the 3 x 3 node coupling pattern."""
     rng = np.random.default_rng(ny * 1000 + nx)
@@ -124,7 +130,7 @@ def test_rectangles_random(mf, ny, nx, d, leaf):
     A = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
     A = A + sp.diags(np.asarray(abs(A).sum(axis=1)).ravel() + 1.0)
     b = rng.standard_normal(n)
-    x, res, As, bs = _solve(mf, d, ny, nx, leaf, A, b)
+    x, res, As, bs = _solve(mf, d, ny, nx, leaf, A, b, inverted)
     assert res < 1e-12, res
 
 
