@@ -22,9 +22,9 @@ import time
 CANDIDATES = {
     "mf_leaf_vector": [16, 24, 32, 48],
     "mf_local_factor_ops": [4, 8, 16, 32],
-    "mf_local_solve_tiles": [12, 24, 48],
+    "mf_local_solve_tiles": [12, 24, 48, 64, 96, 128],
 }
-DEFAULTS = {"mf_leaf_vector": 32, "mf_local_factor_ops": 8, "mf_local_solve_tiles": 24}
+DEFAULTS = {"mf_leaf_vector": 32, "mf_local_factor_ops": 8, "mf_local_solve_tiles": 64}
 
 
 def time_config(make_state, opts, steps, warmup):

@@ -1314,9 +1314,11 @@ static int mf_grid(const erebus_state *s) {
 // fixed cost of the cooperative phases (a grid barrier and a pass over the
 // level's fronts each): the factor runs a front per CTA when that front's
 // tile operations are few, the solve when its tile sweeps are short.  The
-// thresholds come from timing each phase of the 141x141 systems on a B200.
+// thresholds come from timing whole timesteps of the 141x141 and 401x401
+// workloads on a B200 (erebus_b200.autotune): with inverted pivot blocks at
+// the cooperative levels, 64 tiles per sweep beat 24 by 0.7-1.5%.
 constexpr int kLocalFactorOps = 8;    // tile operations per CTA
-constexpr int kLocalSolveTiles = 24;  // tiles streamed per CTA and sweep
+constexpr int kLocalSolveTiles = 64;  // tiles streamed per CTA and sweep
 static std::vector<int> mf_level_modes(const MfPlan &P, int G, int factor_ops,
                                        int solve_tiles) {
     std::vector<int> mode;

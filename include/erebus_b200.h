@@ -210,7 +210,7 @@ typedef struct ErebusSolverOptions {
     int32_t mf_leaf_scalar;       /* the same for the heat and gravity systems (64) */
     int32_t mf_local_factor_ops;  /* a level factors one front per CTA when a CTA's
                                      share is at most this many tile operations (8) */
-    int32_t mf_local_solve_tiles; /* ... and solves so when at most this many tiles (24) */
+    int32_t mf_local_solve_tiles; /* ... and solves so when at most this many tiles (64) */
     /* Levels solved cooperatively (by all CTAs): 0 (default) inverts their
        fronts' pivot blocks after the factorisation, so each triangular
        sweep of a level is two rounds of independent row-block products;
