@@ -220,7 +220,7 @@ int erebus_default_solver_options(ErebusSolverOptions *o) {
     o->krylov = 0;
     o->precond_fp32 = 0;
     o->krylov_restart = 30;
-    o->refactor_iterations = 8;
+    o->refactor_iterations = 0;
     o->mf_leaf_vector = 0;
     o->mf_leaf_scalar = 0;
     o->mf_local_factor_ops = 0;
@@ -430,7 +430,7 @@ int erebus_set_solver_options(erebus_state *s, const ErebusSolverOptions *o) {
         return EREBUS_EINVAL;
     if (o->krylov && (o->direct_solver != EREBUS_SOLVER_MULTIFRONTAL || o->factor_fp32 ||
                       o->krylov_restart < 1 || o->krylov_restart > KRYLOV_MAX_RESTART ||
-                      o->refactor_iterations < 1))
+                      o->refactor_iterations < 0))
         return EREBUS_EINVAL;
     if (o->mf_leaf_vector != s->opt.mf_leaf_vector ||
         o->mf_leaf_scalar != s->opt.mf_leaf_scalar ||

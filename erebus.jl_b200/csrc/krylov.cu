@@ -14,13 +14,20 @@
 //    from an FP32 copy of its FP64 factors (a triangular solve then reads
 //    half the bytes);
 //  * the factors are kept while the matrix changes, and computed again (in
-//    FP64) only when the previous solve of the system needed more than
-//    refactor_iterations iterations, or when a solve reaches three times that
-//    many without converging.
+//    FP64) when they stop paying: by default when the previous solve's cost
+//    reached the average cost per solve since the last factorisation, the
+//    factorisation included (the renewal rule for the cheapest long-run
+//    cost per solve while iterations grow with the preconditioner's age;
+//    the factorisation's cost in iterations comes from a fixed cost model of
+//    the plan, so the decisions, and the results, are the same run to run);
+//    with refactor_iterations = n > 0, when the previous solve needed more
+//    than n iterations.  A solve that reaches three times the break-even
+//    count without converging refactors on the spot.
 //
 // Every reduction is summed in a fixed order (block partials, then the blocks
 // in order), so a solve is reproducible run to run.  The residual targets are
 // the plain path's (hydro_rtol and friends).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -127,6 +134,21 @@ int kalloc(erebus_state *s, BandSystem &sys, int m) {
     return EREBUS_OK;
 }
 
+// Cost of one factorisation of `sys` in Krylov iterations, from the plan:
+// the factorisation as FP64 tile flops at 15 TFLOP/s plus 0.25 ms per tree
+// level, an iteration as the factor bytes one triangular solve reads at
+// 3 TB/s plus 25 us per level plus ~30 FP64 vector passes at 5 TB/s
+// (rates of the multifrontal kernels measured on a B200 at 141x141 and
+// 401x401: 11 and 36 iterations against 14 and 32 from the model).
+double refactor_cost(const erebus_state *s, const BandSystem &sys) {
+    ErebusFactorStats fs = {};
+    mf_stats(s, sys, &fs);
+    const double np = (double)sys.NB * sys.nb;
+    const double tf = fs.flops / 15e12 + fs.levels * 0.25e-3;
+    const double ti = fs.solve_bytes / 3e12 + fs.levels * 25e-6 + np * 8.0 * 30.0 / 5e12;
+    return tf / ti;
+}
+
 // Factor the current matrix in FP64 (and, for the Stokes-Darcy system when
 // precond_fp32 is set, make the FP32 copy its triangular solves read; the
 // scalar systems' solves are short, and their FP64 factors save the extra
@@ -159,10 +181,22 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
     BandView B = band_view(sys);
     const int nb = nblocks(np);
 
+    if (thr == 0 && sys.refactor_cost == 0.0) sys.refactor_cost = refactor_cost(s, sys);
+    // iterations at which the next solve would cost the cycle's average
+    const int even = thr > 0 ? thr
+                             : std::max(4, (int)std::ceil((sys.refactor_cost + sys.cyc_iters) /
+                                                          std::max(1, sys.cyc_solves)));
     timer_begin(s, sys.ph_solve);
-    if (!sys.has_factor || (!sys.factored && sys.last_iterations > thr)) {
+    int at_factor = 0;   // iterations of this solve before its factorisation
+    const bool stale = thr > 0 ? sys.last_iterations > thr
+                               : sys.cyc_solves > 0 &&
+                                     (double)sys.last_iterations * sys.cyc_solves >=
+                                         sys.refactor_cost + sys.cyc_iters;
+    if (!sys.has_factor || (!sys.factored && stale)) {
         rc = refactor(s, sys);
         if (rc) return rc;
+        sys.cyc_solves = 0;
+        sys.cyc_iters = 0;
     }
     if (!sys.have_x) cudaMemsetAsync(sys.x, 0, np * 8, s->stream);
 
@@ -191,6 +225,15 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
             return EREBUS_ENONFINITE;
         }
         if (cycle > 0 && rel > 0.5 * prev_cycle) {   // a whole cycle did not halve it
+            if (!sys.factored) {                      // lagged factors: refresh them
+                rc = refactor(s, sys);
+                if (rc) return rc;
+                sys.cyc_solves = 0;
+                sys.cyc_iters = 0;
+                at_factor = total;
+                prev_cycle = INFINITY;
+                continue;
+            }
             stalled = true;
             break;
         }
@@ -202,11 +245,14 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
             sys.floor_uses++;
             break;
         }
-        if (total >= 3 * thr && !sys.factored) {      // lagged factors no longer pay
+        if (total >= 3 * even && !sys.factored) {     // lagged factors no longer pay
             rc = refactor(s, sys);
             if (rc) return rc;
+            sys.cyc_solves = 0;
+            sys.cyc_iters = 0;
+            at_factor = total;
         }
-        if (total >= 40 * thr) break;
+        if (total >= 40 * std::max(even, 8)) break;
         prev_cycle = rel;
         const double beta = sqrt(rr);
         EREBUS_LAUNCH(s, k_scale, nb, kThreads, 0, V, r, 1.0 / beta, np);
@@ -275,6 +321,8 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
     timer_end(s, sys.ph_solve);
     sys.last_iterations = total;
     sys.krylov_iterations += total;
+    sys.cyc_solves++;
+    sys.cyc_iters += total - at_factor;
     sys.have_x = rel < 1e-6;
     sys.warm_ok = false;
     if (rel <= rtol) {

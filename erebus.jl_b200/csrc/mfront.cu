@@ -74,6 +74,8 @@ struct MfDevice {
     double *vec2 = nullptr, *part = nullptr;
     int2 *inv_list = nullptr;   // (front, Kt) of the fronts k_mf_invert works on
     int n_inv = 0, inv_ktmax = 0;
+    longlong2 *cvt = nullptr;   // storage ranges the FP32 copy converts
+    int n_cvt = 0;
     long long *target = nullptr;
     int *expect = nullptr;
     int nlev = 0;
@@ -1285,12 +1287,16 @@ void mf_release(BandSystem &sys) {
     MfDevice *D = sys.mf;
     if (!D) return;
     void *ps[] = {D->fr, D->F64, D->F32, D->vec, D->vars, D->eamap, D->lvl, D->lvl_kt,
-                  D->lvl_mode, D->flags, D->target, D->expect, D->vec2, D->part, D->inv_list};
+                  D->lvl_mode, D->flags, D->target, D->expect, D->vec2, D->part, D->inv_list,
+                  D->cvt};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete D;
     sys.mf = nullptr;
     sys.has_factor = false;
+    sys.refactor_cost = 0.0;   // the next plan may differ
+    sys.cyc_solves = 0;
+    sys.cyc_iters = 0;
 }
 
 template <class T>
@@ -1512,11 +1518,20 @@ int mf_factor(erebus_state *s, BandSystem &sys, bool fp32) {
     return EREBUS_OK;
 }
 
+// The FP32 copy holds only what the triangular solves read: per front the
+// pivot columns (tile columns J < Kt) and the pivot rows of the other
+// columns (tiles (I, J), I < Kt <= J).  The Schur complement block, which
+// the parent consumed in the extend-add, is not copied.  One CTA per range
+// (x: first element, y: element count, both multiples of 4096).
 __global__ void k_f64_to_f32(const double *__restrict__ src, float *__restrict__ dst,
-                             long long n) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
-        dst[k] = (float)src[k];
+                             const longlong2 *__restrict__ ranges) {
+    const longlong2 r = ranges[blockIdx.x];
+    const double2 *s2 = reinterpret_cast<const double2 *>(src + r.x);
+    float2 *d2 = reinterpret_cast<float2 *>(dst + r.x);
+    for (long long k = threadIdx.x; k < r.y / 2; k += blockDim.x) {
+        const double2 v = __ldcs(&s2[k]);
+        d2[k] = make_float2((float)v.x, (float)v.y);
+    }
 }
 
 int mf_convert_fp32(erebus_state *s, BandSystem &sys) {
@@ -1533,8 +1548,24 @@ int mf_convert_fp32(erebus_state *s, BandSystem &sys) {
             return EREBUS_ENOMEM;
         }
     }
-    EREBUS_LAUNCH(s, k_f64_to_f32, 4 * mf_grid(s), 256, 0, (const double *)D->F64,
-                  (float *)D->F32, (long long)D->plan.storage);
+    if (!D->cvt) {
+        std::vector<longlong2> r;
+        for (const MfFront &F : D->plan.fronts)
+            for (int J = 0; J < F.Mt; J++) {
+                const long long n = J < F.Kt ? F.Mt : F.Kt;
+                if (n > 0)
+                    r.push_back(make_longlong2(F.off + (long long)J * F.Mt * T2, n * T2));
+            }
+        cudaError_t e = upload(&D->cvt, r, s->stream);
+        if (e != cudaSuccess) {
+            s->last_error = std::string("multifrontal FP32 ranges: ") + cudaGetErrorString(e);
+            return EREBUS_ENOMEM;
+        }
+        D->n_cvt = (int)r.size();
+    }
+    if (D->n_cvt > 0)
+        EREBUS_LAUNCH(s, k_f64_to_f32, D->n_cvt, 256, 0, (const double *)D->F64, (float *)D->F32,
+                      (const longlong2 *)D->cvt);
     D->solve32 = true;
     return check_cuda(s, cudaGetLastError(), "mf_convert_fp32");
 }

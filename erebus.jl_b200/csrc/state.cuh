@@ -102,6 +102,9 @@ struct BandSystem {
     bool has_factor = false;       // factors exist (possibly of an earlier matrix)
     int krylov_iterations = 0;     // FGMRES iterations so far
     int last_iterations = 0;       // iterations of this system's previous solve
+    double refactor_cost = 0.0;    // modelled factorisation cost in Krylov iterations (0: not yet)
+    int cyc_solves = 0;            // solves since the last factorisation
+    int cyc_iters = 0;             // their iterations
     int kdim = 0;                  // restart length the basis below was allocated for
     double *kbasis = nullptr;      // V (kdim + 1 vectors) then Z (kdim vectors), np each
     double *kwork = nullptr;       // dot partials, h, y (device)

@@ -191,9 +191,15 @@ typedef struct ErebusSolverOptions {
        (residuals, matrix products, orthogonalisation, the solution update)
        preconditioned by the multifrontal LU factors.  The factors are kept
        as the preconditioner after the matrix changes and computed again (in
-       FP64) only when the previous solve of the system needed more than
-       refactor_iterations Krylov iterations, or when a solve reaches
-       3 x refactor_iterations without converging.  With precond_fp32 = 1 the
+       FP64) when they stop paying.  With refactor_iterations = 0 (default)
+       that is when the previous solve's iterations times the solves since
+       the last factorisation reach the factorisation's cost (modelled from
+       the plan, in iterations) plus those solves' iterations, i.e. when a
+       solve costs as much as the average solve since the factorisation,
+       the factorisation included; with refactor_iterations = n > 0, when
+       the previous solve needed more than n iterations.  A solve that
+       reaches three times that break-even count without converging
+       refactors on the spot.  With precond_fp32 = 1 the
        Stokes-Darcy preconditioner is applied from an FP32 copy of those FP64
        factors (half the bytes per triangular solve); the heat and gravity
        systems, whose solves are short, keep applying FP64 factors.  The
@@ -201,7 +207,7 @@ typedef struct ErebusSolverOptions {
     int32_t krylov;            /* 1: FGMRES with lagged LU preconditioner */
     int32_t precond_fp32;      /* 1: apply the preconditioner from FP32 factors */
     int32_t krylov_restart;    /* FGMRES restart length (1..64) */
-    int32_t refactor_iterations; /* refresh the factors after a solve that took more */
+    int32_t refactor_iterations; /* 0: cost rule above; n > 0: after a solve that took more than n */
     /* Multifrontal analysis (no reference counterpart), 0 = the built-in
        default; erebus_b200.autotune picks them per grid size by timing.
        Changing them takes effect at the next analysis (a new state, or a

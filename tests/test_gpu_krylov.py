@@ -3,8 +3,10 @@
 With ErebusSolverOptions.krylov = 1 every solve is a flexible GMRES in FP64
 preconditioned by the multifrontal LU of an earlier matrix of the same
 system, applied from an FP32 copy of its FP64 factors (precond_fp32 = 1);
-the factors are refreshed only when a solve needed more than
-refactor_iterations iterations.  The solves meet the plain path's residual
+the factors are refreshed when a solve costs as much as the average solve
+since the last factorisation, the factorisation included (its cost in
+iterations modelled from the plan), or with refactor_iterations = n > 0
+when a solve needed more than n iterations.  The solves meet the plain path's residual
 target (1e-13), so the results agree with the oracle's SuperLU solves to the
 same tolerances as the plain path (1e-8 relative L2 per field, marker
 positions 1e-10), and with the plain FP64 GPU path to 1e-8.
@@ -102,3 +104,18 @@ def test_krylov_lagged_factors_141(pkg, built_lib):
         assert rel_l2(a.grid[k], b.grid[k]) < 1e-8, k
         np.testing.assert_array_equal(a.grid[k], c.grid[k])
     assert max(s.worst_rel_residual for s in sa) <= 1e-10
+
+
+def test_krylov_fixed_refactor_threshold(pkg, built_lib):
+    """The fixed-threshold rule (refactor_iterations = 4) on the 141 x 141
+    workload: it factors at least as often as the cost rule and ends at the
+    same state to the solve tolerance."""
+    a, sa, fa = _run(pkg, "planetesimal_141", 4, **MIXED)
+    b, sb, fb = _run(pkg, "planetesimal_141", 4, refactor_iterations=4, **MIXED)
+    assert fb.factorizations >= fa.factorizations
+    assert [s.titer for s in sa] == [s.titer for s in sb]
+    n = a.marknum
+    for k in ("xm", "ym"):
+        assert rel_linf(a.m[k][:n], b.m[k][:n]) < 1e-10, k
+    for k in ("tk2", "pr", "pf", "vx", "vy"):
+        assert rel_l2(a.grid[k], b.grid[k]) < 1e-8, k
