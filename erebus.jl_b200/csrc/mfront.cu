@@ -243,6 +243,10 @@ constexpr int MF_KM_MAX = 256;
 // Bits of MfView::lvl_mode: the level runs one front per CTA in the factor /
 // in the solve (else cooperatively, tile tasks dealt over all CTAs).
 constexpr int MF_FACTOR_LOCAL = 1, MF_SOLVE_LOCAL = 2;
+// ... and every front of the level keeps its vector in shared memory
+// (M <= MF_VS_MAX), so the level's sweeps stream all of a CTA's fronts
+// through one tile pipeline.
+constexpr int MF_SOLVE_VS = 4;
 
 struct MfFactorSmem {
     MmaSmem m;
@@ -522,6 +526,16 @@ static_assert(sizeof(MfSolveSmem) <= 113 * 1024, "solve shared memory");
 
 __device__ __forceinline__ uint32_t mf_smem(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Tile slots in flight per CTA (three for either element type: six FP32
+// slots in the same storage measured no faster) and slot sl's tile.
+template <class T> struct MfSlots {
+    static constexpr int n = MF_SLOTS;
+};
+template <class T>
+__device__ __forceinline__ const T *mf_slot(MfSolveSmem &S, int sl) {
+    return reinterpret_cast<const T *>(S.tile[sl]);
 }
 
 // Issues the copy of one 64 x 64 tile into slot `sl` (thread 0).
@@ -900,6 +914,246 @@ __device__ void mf_bwd_front_s(const MfView &V, const MfFront &f, double *w, MfS
     __syncthreads();
 }
 
+// ---- one front per CTA, a level at a time -----------------------------------
+// The sweeps of mf_fwd_front_s / mf_bwd_front_s (same arithmetic, same
+// order) over all of this CTA's fronts of a level (fronts fb + blockIdx.x +
+// k G) through one tile pipeline: thread 0 keeps a fetch cursor that runs
+// MfSlots<T>::n tiles ahead across the fronts, so the next front's first
+// tiles are in flight while the current front finishes and the next one is
+// gathered.
+
+// Fetch cursor of the forward sweep: tiles (I, K), K < Kt, I = K+1..Mt-1.
+template <class T>
+struct MfFwdCursor {
+    int fi, fe, G, K, I, Kt, Mt;
+    long long off;
+    __device__ void load(const MfView &V) {
+        if (fi < fe) {
+            const MfFront &F = V.fr[fi];
+            off = F.off;
+            Kt = F.Kt;
+            Mt = F.Mt;
+            K = 0;
+            I = 1;
+        }
+    }
+    __device__ const T *next(const MfView &V) {
+        while (fi < fe) {
+            while (K < Kt && I >= Mt) {
+                K++;
+                I = K + 1;
+            }
+            if (K < Kt) return (const T *)V.F + off + ((long long)K * Mt + I++) * T2;
+            fi += G;
+            load(V);
+        }
+        return nullptr;
+    }
+};
+
+// Fetch cursor of the backward sweep: the ring tiles (K, Kt + j) row by row,
+// then (K, K), (0, K), ..., (K-1, K) for K = Kt-1 .. 0.
+template <class T>
+struct MfBwdCursor {
+    int fi, fe, G, K, j, ring, Kt, Mt;
+    long long off;
+    __device__ void load(const MfView &V) {
+        if (fi < fe) {
+            const MfFront &F = V.fr[fi];
+            off = F.off;
+            Kt = F.Kt;
+            Mt = F.Mt;
+            ring = Mt > Kt;
+            K = ring ? 0 : Kt - 1;
+            j = 0;
+        }
+    }
+    __device__ const T *next(const MfView &V) {
+        while (fi < fe) {
+            if (ring) {
+                const int nr = Mt - Kt;
+                if (j >= nr) {
+                    j = 0;
+                    K++;
+                }
+                if (K < Kt) {
+                    const int J = Kt + j++;
+                    return (const T *)V.F + off + ((long long)J * Mt + K) * T2;
+                }
+                ring = 0;
+                K = Kt - 1;
+                j = 0;
+            }
+            if (K >= 0 && j > K) {
+                K--;
+                j = 0;
+            }
+            if (K >= 0) {
+                const int I = j == 0 ? K : j - 1;
+                j++;
+                return (const T *)V.F + off + ((long long)K * Mt + I) * T2;
+            }
+            fi += G;
+            load(V);
+        }
+        return nullptr;
+    }
+};
+
+template <class T>
+__device__ void mf_fwd_level_s(const MfView &V, int fb, int fe, const double *w, MfSolveSmem &S,
+                               uint32_t *uses, int *err) {
+    constexpr int NS = MfSlots<T>::n;
+    const int G = gridDim.x;
+    double *vs = S.vs;
+    MfFwdCursor<T> cur;
+    if (threadIdx.x == 0) {
+        cur.fi = fb + blockIdx.x;
+        cur.fe = fe;
+        cur.G = G;
+        cur.load(V);
+        for (int q = 0; q < NS; q++) {
+            const T *p = cur.next(V);
+            if (!p) break;
+            mf_fetch(S, q, p);
+        }
+    }
+    int sl = 0;
+    for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
+        const MfFront f = V.fr[fi];
+        {
+            const int *var = V.vars + f.var_off, *map = V.eamap + f.map_off;
+            MfFront C0, C1;
+            const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
+            if (h0) C0 = V.fr[f.c0];
+            if (h1) C1 = V.fr[f.c1];
+            for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
+                int g = var[a];
+                double s = (a < f.Kp && g >= 0) ? __ldcg(&w[g]) : 0.0;
+                if (h0) {
+                    int i = map[2 * a];
+                    if (i >= 0) s += __ldcg(&V.vec[C0.vec_off + C0.Kp + i]);
+                }
+                if (h1) {
+                    int i = map[2 * a + 1];
+                    if (i >= 0) s += __ldcg(&V.vec[C1.vec_off + C1.Kp + i]);
+                }
+                vs[a] = s;
+            }
+        }
+        __syncthreads();
+        int n = 0;
+        for (int K = 0; K < f.Kt; K++) n += f.Mt - K - 1;
+        int K = 0, I = 1, b = 0;
+        for (int t = 0; t < n; t++) {
+            while (I >= f.Mt) {
+                K++;
+                I = K + 1;
+            }
+            if (I == K + 1) __syncthreads();   // row K is final
+            mf_slot_wait(S, sl, uses[sl] & 1u, err);
+            uses[sl]++;
+            const double r = mf_reduce_rows1(S, mf_quarter(mf_slot<T>(S, sl), vs + K * 64), b);
+            b ^= 1;
+            if (threadIdx.x < 64) vs[I * 64 + threadIdx.x] -= r;
+            if (threadIdx.x == 0) {   // every thread has read the slot (the barrier above)
+                const T *p = cur.next(V);
+                if (p) mf_fetch(S, sl, p);
+            }
+            sl = sl + 1 == NS ? 0 : sl + 1;
+            I++;
+        }
+        __syncthreads();
+        double *v = V.vec + f.vec_off;
+        for (int a = threadIdx.x; a < f.M; a += blockDim.x) __stcg(&v[a], vs[a]);
+        __syncthreads();
+    }
+}
+
+template <class T>
+__device__ void mf_bwd_level_s(const MfView &V, int fb, int fe, double *w, MfSolveSmem &S,
+                               uint32_t *uses, int *err) {
+    constexpr int NS = MfSlots<T>::n;
+    const int G = gridDim.x;
+    double *vs = S.vs;
+    MfBwdCursor<T> cur;
+    if (threadIdx.x == 0) {
+        cur.fi = fb + blockIdx.x;
+        cur.fe = fe;
+        cur.G = G;
+        cur.load(V);
+        for (int q = 0; q < NS; q++) {
+            const T *p = cur.next(V);
+            if (!p) break;
+            mf_fetch(S, q, p);
+        }
+    }
+    int sl = 0;
+    auto refill = [&]() {   // call after a barrier that follows every read of slot sl
+        if (threadIdx.x == 0) {
+            const T *p = cur.next(V);
+            if (p) mf_fetch(S, sl, p);
+        }
+        sl = sl + 1 == NS ? 0 : sl + 1;
+    };
+    for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
+        const MfFront f = V.fr[fi];
+        double *v = V.vec + f.vec_off;
+        const int *var = V.vars + f.var_off;
+        for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
+            if (a < f.Kp) {
+                vs[a] = __ldcg(&v[a]);
+            } else {
+                int g = var[a];
+                vs[a] = g >= 0 ? __ldcg(&w[g]) : 0.0;
+            }
+        }
+        __syncthreads();
+        const int nr = f.Mt - f.Kt;
+        if (nr > 0) {   // rows K < Kt minus the ring products
+            for (int K = 0; K < f.Kt; K++) {
+                double acc = 0.0;
+                for (int j = 0; j < nr; j++) {
+                    mf_slot_wait(S, sl, uses[sl] & 1u, err);
+                    uses[sl]++;
+                    acc += mf_quarter(mf_slot<T>(S, sl), vs + (f.Kt + j) * 64);
+                    __syncthreads();
+                    refill();
+                }
+                const double t = mf_reduce_rows(S, acc);
+                if (threadIdx.x < 64) vs[K * 64 + threadIdx.x] -= t;
+            }
+        }
+        int b = 0;
+        for (int K = f.Kt - 1; K >= 0; K--) {
+            for (int j = 0; j <= K; j++) {
+                mf_slot_wait(S, sl, uses[sl] & 1u, err);
+                uses[sl]++;
+                const T *Tt = mf_slot<T>(S, sl);
+                if (j == 0) {   // x_K = D_K^{-1} v_K
+                    __syncthreads();   // row K is final
+                    const double x = mf_reduce_rows1(S, mf_quarter(Tt, vs + K * 64), b);
+                    if (threadIdx.x < 64) {
+                        const int r = threadIdx.x, a = K * 64 + r;
+                        S.x[r] = x;
+                        vs[a] = x;
+                        __stcg(&v[a], x);
+                        if (a < f.k) __stcg(&w[var[a]], x);
+                    }
+                    refill();
+                    __syncthreads();   // S.x is complete
+                } else {        // v_I -= U_IK x_K, I = j - 1
+                    const double t = mf_reduce_rows1(S, mf_quarter(Tt, S.x), b);
+                    if (threadIdx.x < 64) vs[(j - 1) * 64 + threadIdx.x] -= t;
+                    refill();
+                }
+                b ^= 1;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // ---- cooperative levels: one task per 64-row block of a front --------------
 // Row block I of front f is final in solve `epoch` once its flag holds
 // 2 epoch (forward) or 2 epoch + 1 (backward); epochs grow, so older marks
@@ -1182,7 +1436,9 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
         const int fb = V.lvl[p], fe = V.lvl[p + 1];
         const bool local = V.lvl_mode[p] & MF_SOLVE_LOCAL;
         if (!local) mf_load_km(V, fb, fe, S.km);
-        if (local) {
+        if (local && (V.lvl_mode[p] & MF_SOLVE_VS)) {
+            mf_fwd_level_s<T>(V, fb, fe, w, S, uses, err);
+        } else if (local) {
             for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
                 const MfFront f = V.fr[fi];
                 if (f.M <= MF_VS_MAX) {
@@ -1221,7 +1477,9 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
                 return g >= 0 ? __ldcg(&w[g]) : 0.0;
             };
         };
-        if (local) {
+        if (local && (V.lvl_mode[p] & MF_SOLVE_VS)) {
+            mf_bwd_level_s<T>(V, fb, fe, w, S, uses, err);
+        } else if (local) {
             for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
                 const MfFront f = V.fr[fi];
                 if (f.M <= MF_VS_MAX) {
@@ -1348,6 +1606,9 @@ static std::vector<int> mf_level_modes(const MfPlan &P, int G, int factor_ops,
         }
         const bool forced = F >= G / 2 || F > MF_KM_MAX;
         int m = 0;
+        bool vs = true;
+        for (int fi = fb; fi < fe; fi++) vs = vs && P.fronts[fi].M <= MF_VS_MAX;
+        if (vs) m |= MF_SOLVE_VS;
         if (forced || waves * ops <= factor_ops) m |= MF_FACTOR_LOCAL;
         if (forced || waves * tiles <= solve_tiles) m |= MF_SOLVE_LOCAL;
         mode.push_back(m);
