@@ -373,6 +373,7 @@ def time_mode(pkg, args, mode, world, rank, local, clocks=False):
     f0 = {k: sim.factor_stats(i) for i, k in enumerate(("hydro", "thermal", "gravity"))}
     sim.enable_phase_timing(True)
     l0 = sim.kernel_launches()
+    y0 = sim.host_syncs()
     stream = torch.cuda.ExternalStream(sim.stream_handle())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ck = Clocks(local) if clocks and rank == 0 else None
@@ -391,7 +392,8 @@ def time_mode(pkg, args, mode, world, rank, local, clocks=False):
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, world)
     out = {"ms": ms_max, "value": world * args.steps / (ms_max / 1000.0), "stats": stats,
-           "launches": sim.kernel_launches() - l0, "phases": sim.phase_times(),
+           "launches": sim.kernel_launches() - l0, "host_syncs": sim.host_syncs() - y0,
+           "phases": sim.phase_times(),
            "fstats": {k: sim.factor_stats(i)
                       for i, k in enumerate(("hydro", "thermal", "gravity"))},
            "clocks": ck, "marknum": st.marknum}
@@ -528,7 +530,8 @@ def run_ours(args):
                     "hydro_solves": sum(s.hydro_solves for s in r["stats"]),
                     "worst_rel_residual": max(s.worst_rel_residual for s in r["stats"]),
                     "solver_options": MODES[mode], "phases": r["per"],
-                    "gpu_launches": r["launches"]}
+                    "gpu_launches": r["launches"],
+                    "host_syncs_per_step": r["host_syncs"] / args.steps}
         line = {"metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": h["ms"] / args.steps, "higher_is_better": True,

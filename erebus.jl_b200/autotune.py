@@ -1,9 +1,9 @@
 """Autotuner of the multifrontal solver's analysis parameters.
 
-The nested-dissection leaf size and the thresholds that decide, per tree
+The nested-dissection leaf sizes and the thresholds that decide, per tree
 level, whether a CTA takes a whole front or the front's tiles are dealt to
-all CTAs (ErebusSolverOptions.mf_leaf_vector, mf_local_factor_ops,
-mf_local_solve_tiles) trade tree depth against tile work and the fixed cost
+all CTAs (ErebusSolverOptions.mf_leaf_vector, mf_leaf_scalar,
+mf_local_factor_ops, mf_local_solve_tiles) trade tree depth against tile work and the fixed cost
 of cooperative phases; the best values depend on the grid size.  `tune`
 picks them by timing whole timesteps on the device (coordinate descent over
 candidate values, each trial from the same initial state), and `main` runs
@@ -21,10 +21,12 @@ import time
 
 CANDIDATES = {
     "mf_leaf_vector": [16, 24, 32, 48],
+    "mf_leaf_scalar": [32, 64, 128, 256],
     "mf_local_factor_ops": [4, 8, 16, 32],
     "mf_local_solve_tiles": [12, 24, 48, 64, 96, 128],
 }
-DEFAULTS = {"mf_leaf_vector": 32, "mf_local_factor_ops": 8, "mf_local_solve_tiles": 64}
+DEFAULTS = {"mf_leaf_vector": 32, "mf_leaf_scalar": 64, "mf_local_factor_ops": 8,
+            "mf_local_solve_tiles": 64}
 
 
 def time_config(make_state, opts, steps, warmup):

@@ -374,7 +374,7 @@ int fail_adj(erebus_state *s, const char *msg) {
 int read_flag(erebus_state *s, int *flag, int *out) {
     ATRY(check_cuda(s, cudaMemcpyAsync(out, flag, sizeof(int), cudaMemcpyDeviceToHost,
                                        s->stream), "adjoint flag"));
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "adjoint flag");
+    return stream_sync(s, "adjoint flag");
 }
 
 }  // namespace
@@ -553,7 +553,7 @@ extern "C" int erebus_adjoint_heat(erebus_state *s, int32_t first_timestep, int3
     if (dJ_dphim)
         ATRY(check_cuda(s, cudaMemcpyAsync(dJ_dphim, L.phibar, n * 8, cudaMemcpyDeviceToHost,
                                            s->stream), "adjoint"));
-    ATRY(check_cuda(s, cudaStreamSynchronize(s->stream), "adjoint"));
+    ATRY(stream_sync(s, "adjoint"));
     double Jv = host_out[0] / (double)nbody;
     if (J) *J = Jv;
     if (dJ_dratio_al) *dJ_dratio_al = host_out[1];

@@ -21,6 +21,11 @@ int check_cuda(erebus_state *s, cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? EREBUS_ENOMEM : EREBUS_ECUDA;
 }
 
+int stream_sync(erebus_state *s, const char *what) {
+    s->host_syncs++;
+    return check_cuda(s, cudaStreamSynchronize(s->stream), what);
+}
+
 static cudaEvent_t timer_event(erebus_state *s) {
     if (!s->ev_pool.empty()) {
         cudaEvent_t e = s->ev_pool.back();
@@ -259,6 +264,7 @@ int erebus_destroy(erebus_state *s) {
     if (s->adj_mem) cudaFree(s->adj_mem);
     if (s->hsc) cudaFreeHost(s->hsc);
     if (s->copy_stream) {
+        s->host_syncs++;
         cudaStreamSynchronize(s->copy_stream);
         cudaStreamDestroy(s->copy_stream);
         cudaEventDestroy(s->snap_ready);
@@ -477,7 +483,7 @@ int erebus_upload_markers(erebus_state *s, const ErebusMarkersHost *m, int64_t m
     }
     TRY(check_cuda(s, cudaMemcpyAsync(s->tm8, t.data(), marknum, cudaMemcpyHostToDevice,
                                       s->stream), "upload tm"));
-    TRY(check_cuda(s, cudaStreamSynchronize(s->stream), "upload"));
+    TRY(stream_sync(s, "upload"));
     s->marknum = marknum;
     s->sorted_valid = false;
     return EREBUS_OK;
@@ -496,7 +502,7 @@ int erebus_download_markers(erebus_state *s, ErebusMarkersHost *m, int64_t *mark
     std::vector<int8_t> t(n);
     TRY(check_cuda(s, cudaMemcpyAsync(t.data(), s->tm8, n, cudaMemcpyDeviceToHost, s->stream),
                    "download tm"));
-    TRY(check_cuda(s, cudaStreamSynchronize(s->stream), "download"));
+    TRY(stream_sync(s, "download"));
     if (m->tm)
         for (int64_t k = 0; k < n; k++) m->tm[k] = t[k];
     if (marknum) *marknum = n;
@@ -517,7 +523,7 @@ int erebus_upload_grid(erebus_state *s, const ErebusGridHost *gh) {
         TRY(check_cuda(s, cudaMemcpyAsync(s->grid[f], src[f], field_bytes(s, f),
                                           cudaMemcpyHostToDevice, s->stream), "upload grid"));
     }
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "upload grid");
+    return stream_sync(s, "upload grid");
 }
 
 int erebus_download_grid(erebus_state *s, ErebusGridHost *gh) {
@@ -529,7 +535,7 @@ int erebus_download_grid(erebus_state *s, ErebusGridHost *gh) {
         TRY(check_cuda(s, cudaMemcpyAsync(dst[f], s->grid[f], field_bytes(s, f),
                                           cudaMemcpyDeviceToHost, s->stream), "download grid"));
     }
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "download grid");
+    return stream_sync(s, "download grid");
 }
 
 int erebus_download_sums(erebus_state *s, ErebusSumsHost *sh) {
@@ -542,7 +548,7 @@ int erebus_download_sums(erebus_state *s, ErebusSumsHost *sh) {
         TRY(check_cuda(s, cudaMemcpyAsync(dst[f], s->sums[f], n * 8, cudaMemcpyDeviceToHost,
                                           s->stream), "download sums"));
     }
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "download sums");
+    return stream_sync(s, "download sums");
 }
 
 // save_state (E:5718-5960) every savematstep timesteps (E:7106): the state is
@@ -660,6 +666,12 @@ int erebus_kernel_launches(const erebus_state *s, int64_t *count) {
     return EREBUS_OK;
 }
 
+int erebus_host_syncs(const erebus_state *s, int64_t *count) {
+    if (!s || !count) return EREBUS_EINVAL;
+    *count = s->host_syncs;
+    return EREBUS_OK;
+}
+
 int erebus_get_stream(const erebus_state *s, void **stream) {
     if (!s || !stream) return EREBUS_EINVAL;
     *stream = (void *)s->stream;
@@ -701,7 +713,7 @@ static int set_dev_dt(erebus_state *s, double dt) {
 static int read_scalars(erebus_state *s) {
     TRY(check_cuda(s, cudaMemcpyAsync(s->hsc, s->dsc, sizeof(DevScalars),
                                       cudaMemcpyDeviceToHost, s->stream), "scalars"));
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "scalars");
+    return stream_sync(s, "scalars");
 }
 
 static double slot(const erebus_state *s, int k) { return s->hsc->maxabs[k]; }
@@ -719,7 +731,7 @@ int erebus_markers_to_nodes(erebus_state *s, double timesum) {
     if (!s) return EREBUS_EINVAL;
     cudaSetDevice(s->device);
     TRY(markers_to_nodes(s, timesum));
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "markers_to_nodes");
+    return stream_sync(s, "markers_to_nodes");
 }
 
 int erebus_gravity(erebus_state *s, ErebusSolveStats *st) {
@@ -731,7 +743,7 @@ int erebus_gravity(erebus_state *s, ErebusSolveStats *st) {
     TRY(check_cuda(s, cudaMemcpyAsync(s->grid[G_FI], s->gravity.x, np * 8,
                                       cudaMemcpyDeviceToDevice, s->stream), "FI"));
     TRY(gravity_post(s));
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "gravity");
+    return stream_sync(s, "gravity");
 }
 
 int erebus_thermochemical_reaction(erebus_state *s, double dt, int32_t timestep,
@@ -739,7 +751,7 @@ int erebus_thermochemical_reaction(erebus_state *s, double dt, int32_t timestep,
     if (!s) return EREBUS_EINVAL;
     cudaSetDevice(s->device);
     TRY(thermochemical_reaction(s, dt, timestep, titer));
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "reaction");
+    return stream_sync(s, "reaction");
 }
 
 int erebus_hydromech_pass(erebus_state *s, double *dt, int32_t iplast, int32_t *converged,
@@ -768,7 +780,7 @@ int erebus_hydromech_pass(erebus_state *s, double *dt, int32_t iplast, int32_t *
     }
     *dt = d;
     if (converged) *converged = conv;
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "hydromech_pass");
+    return stream_sync(s, "hydromech_pass");
 }
 
 int erebus_thermal_solve(erebus_state *s, double dt, int32_t timestep, double *maxDT,
@@ -799,7 +811,7 @@ int erebus_nodes_to_markers(erebus_state *s, double dt, int32_t timestep) {
     if (!s) return EREBUS_EINVAL;
     cudaSetDevice(s->device);
     TRY(nodes_to_markers(s, dt, timestep));
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "nodes_to_markers");
+    return stream_sync(s, "nodes_to_markers");
 }
 
 int erebus_advect_rk4(erebus_state *s, double dt) {
@@ -807,7 +819,7 @@ int erebus_advect_rk4(erebus_state *s, double dt) {
     cudaSetDevice(s->device);
     TRY(velocities_rotation(s));
     TRY(advect(s, dt));
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "advect");
+    return stream_sync(s, "advect");
 }
 
 int erebus_replenish(erebus_state *s, int32_t timestep, int64_t *marknum) {
@@ -1021,7 +1033,7 @@ int erebus_step_host(erebus_state *s, int32_t timestep, const ErebusMarkersHost 
     int bad = 0;
     TRY(check_cuda(s, cudaMemcpyAsync(&bad, &s->dsc->err, sizeof(int), cudaMemcpyDeviceToHost,
                                       s->stream), "step_host"));
-    TRY(check_cuda(s, cudaStreamSynchronize(s->stream), "step_host"));
+    TRY(stream_sync(s, "step_host"));
     if (bad) {
         s->last_error = "step_host: marker type outside 1..3";
         return EREBUS_EINVAL;
@@ -1033,6 +1045,7 @@ int erebus_step_host(erebus_state *s, int32_t timestep, const ErebusMarkersHost 
     ErebusStepStats stats = {};
     int rc = step_impl(s, timestep, &stats, early_copies, &ctx);
     if (rc) {
+        s->host_syncs++;
         cudaStreamSynchronize(s->copy_stream);
         return rc;
     }
@@ -1053,8 +1066,9 @@ int erebus_step_host(erebus_state *s, int32_t timestep, const ErebusMarkersHost 
                        "step_host"));
     }
     TRY(copy_grid(s, s->grid[0], (const void *const *)gdst, cudaMemcpyDeviceToHost));
+    s->host_syncs++;
     TRY(check_cuda(s, cudaStreamSynchronize(s->copy_stream), "step_host"));
-    TRY(check_cuda(s, cudaStreamSynchronize(s->stream), "step_host"));
+    TRY(stream_sync(s, "step_host"));
     if (marknum_out) *marknum_out = n2;
     if (st) *st = stats;
     return EREBUS_OK;
@@ -1086,7 +1100,7 @@ int erebus_apply_hydromech(erebus_state *s, double dt, const double *x, double *
     (void)B;
     TRY(band_apply_unscaled(s, sys, dx, dy));
     cudaMemcpyAsync(y, dy, n * 8, cudaMemcpyDeviceToHost, s->stream);
-    int rc = check_cuda(s, cudaStreamSynchronize(s->stream), "apply");
+    int rc = stream_sync(s, "apply");
     cudaFreeAsync(dx, s->stream);
     cudaFreeAsync(dy, s->stream);
     return rc;

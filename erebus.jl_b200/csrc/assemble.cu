@@ -336,7 +336,7 @@ int assemble_system(erebus_state *s, int kind) {
     int rc = check_cuda(s, cudaMemcpyAsync(&changed, sys.changed, sizeof(int),
                                            cudaMemcpyDeviceToHost, s->stream), "assemble");
     if (rc) return rc;
-    rc = check_cuda(s, cudaStreamSynchronize(s->stream), "assemble");
+    rc = stream_sync(s, "assemble");
     if (rc) return rc;
     if (changed || !sys.factored || !s->opt.reuse_factors) {
         rc = commit_assembly(s, sys);
@@ -384,7 +384,7 @@ int export_system(erebus_state *s, int kind, int64_t *nnz_out, int64_t *rows_h,
     cudaMemcpyAsync(c.data(), dc, n * 12 * 8, cudaMemcpyDeviceToHost, s->stream);
     cudaMemcpyAsync(v.data(), dv, n * 12 * 8, cudaMemcpyDeviceToHost, s->stream);
     if (rhs_h) cudaMemcpyAsync(rhs_h, db, n * 8, cudaMemcpyDeviceToHost, s->stream);
-    rc = check_cuda(s, cudaStreamSynchronize(s->stream), "export");
+    rc = stream_sync(s, "export");
     cudaFreeAsync(dr, s->stream);
     cudaFreeAsync(dc, s->stream);
     cudaFreeAsync(dv, s->stream);

@@ -577,7 +577,7 @@ int mf_check_error(erebus_state *s, BandSystem &sys, const char *what) {
     int rc = check_cuda(s, cudaMemcpyAsync(&h, sys.err, sizeof(int), cudaMemcpyDeviceToHost,
                                            s->stream), what);
     if (rc) return rc;
-    rc = check_cuda(s, cudaStreamSynchronize(s->stream), what);
+    rc = stream_sync(s, what);
     if (rc) return rc;
     if (h) {
         s->last_error = std::string(what) +

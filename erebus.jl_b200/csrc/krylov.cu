@@ -120,12 +120,15 @@ int kalloc(erebus_state *s, BandSystem &sys, int m) {
     if (sys.kbasis && sys.kdim >= m) return EREBUS_OK;
     if (sys.kbasis) cudaFree(sys.kbasis);
     if (sys.kwork) cudaFree(sys.kwork);
+    if (sys.khost) cudaFreeHost(sys.khost);
     sys.kbasis = nullptr;
     sys.kwork = nullptr;
+    sys.khost = nullptr;
     const int64_t np = (int64_t)sys.NB * sys.nb;
     cudaError_t e = cudaMalloc(&sys.kbasis, (size_t)(2 * m + 1) * np * sizeof(double));
     if (e == cudaSuccess)
         e = cudaMalloc(&sys.kwork, (size_t)(KB * (m + 2) + 4 * (m + 2)) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&sys.khost, (size_t)(2 * m + 2) * sizeof(double));
     if (e != cudaSuccess) {
         s->last_error = std::string("krylov basis: ") + cudaGetErrorString(e);
         return EREBUS_ENOMEM;
@@ -200,7 +203,10 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
     }
     if (!sys.have_x) cudaMemsetAsync(sys.x, 0, np * 8, s->stream);
 
-    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hh(m + 2);
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1);
+    // page-locked, so the copies of the Hessenberg column and of the update
+    // coefficients are asynchronous (one host wait per iteration)
+    double *hh = sys.khost, *y = sys.khost + (m + 2);
     double *r = sys.r;                             // residual work vector
     int total = 0;
     double rel = INFINITY, prev_cycle = INFINITY, bnorm = 0.0;
@@ -276,12 +282,12 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
             EREBUS_LAUNCH(s, k_maxpy, nb, kThreads, 0, W, V, np, j + 1, h2, -1.0, np);
             EREBUS_LAUNCH(s, k_mdot_part, KB, KT, 0, W, np, 1, W, np, part);
             EREBUS_LAUNCH(s, k_mdot_sum, 1, KT, 0, part, nd, (double *)nullptr);
-            rc = check_cuda(s, cudaMemcpyAsync(hh.data(), hd, (j + 1) * 8,
+            rc = check_cuda(s, cudaMemcpyAsync(hh, hd, (j + 1) * 8,
                                                cudaMemcpyDeviceToHost, s->stream), "krylov h");
             if (!rc) rc = check_cuda(s, cudaMemcpyAsync(&hh[j + 1], nd, 8,
                                                         cudaMemcpyDeviceToHost, s->stream),
                                      "krylov h");
-            if (!rc) rc = check_cuda(s, cudaStreamSynchronize(s->stream), "krylov h");
+            if (!rc) rc = stream_sync(s, "krylov h");
             if (rc) return rc;
             total++;
             const double wn = sqrt(hh[j + 1]);
@@ -310,12 +316,12 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
             for (int c = i + 1; c < j; c++) t -= H[(size_t)i * m + c] * y[c];
             y[i] = t / H[(size_t)i * m + i];
         }
-        rc = check_cuda(s, cudaMemcpyAsync(yd, y.data(), j * 8, cudaMemcpyHostToDevice,
+        rc = check_cuda(s, cudaMemcpyAsync(yd, y, j * 8, cudaMemcpyHostToDevice,
                                            s->stream), "krylov y");
         if (rc) return rc;
         EREBUS_LAUNCH(s, k_maxpy, nb, kThreads, 0, sys.x, Z, np, j, yd, 1.0, np);
         // the host vector y is read by the copy above before it is reused
-        rc = check_cuda(s, cudaStreamSynchronize(s->stream), "krylov update");
+        rc = stream_sync(s, "krylov update");
         if (rc) return rc;
     }
     timer_end(s, sys.ph_solve);
@@ -350,8 +356,10 @@ int krylov_solve(erebus_state *s, BandSystem &sys, double rtol, ErebusSolveStats
 void krylov_free(BandSystem &sys) {
     if (sys.kbasis) cudaFree(sys.kbasis);
     if (sys.kwork) cudaFree(sys.kwork);
+    if (sys.khost) cudaFreeHost(sys.khost);
     sys.kbasis = nullptr;
     sys.kwork = nullptr;
+    sys.khost = nullptr;
     sys.kdim = 0;
 }
 

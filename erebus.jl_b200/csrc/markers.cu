@@ -1283,7 +1283,7 @@ int replenish(erebus_state *s, int timestep, int64_t *marknum) {
                                            sizeof(int), cudaMemcpyDeviceToHost, s->stream),
                         "replenish count");
     if (rc) return rc;
-    rc = check_cuda(s, cudaStreamSynchronize(s->stream), "replenish");
+    rc = stream_sync(s, "replenish");
     if (rc) return rc;
     int add = s->hsc->repl_count;
     if ((int64_t)n + add > s->capacity) {

@@ -1293,13 +1293,47 @@ __device__ void mf_bwd_row(const MfView &V, const MfFront &f, double *w, int K, 
 // x_K = D_K^{-1} t_K - sum_{J>K} Z_KJ t_J with t_J = y_J minus its partials.
 // v is gathered where it is read (children's update parts and the right-
 // hand side), so each sweep of a level takes two phases, and every task is
-// one row block: no task waits for another inside a phase.
+// one row block or a chunk of one: no task waits for another inside a phase.
 constexpr int MF_XG = MF_VS_MAX / 64;    // vector pieces staged in shared memory at a time
 constexpr int MF_RING_CHUNK = MF_XG;      // ring tiles per backward partial sum
 static_assert(MF_XG * 64 == 4 * LU_THREADS, "staging: four elements per thread");
 
 __host__ __device__ __forceinline__ int mf_ring_chunks(int nr) {
     return (nr + MF_RING_CHUNK - 1) / MF_RING_CHUNK;
+}
+
+// F1 splits pivot row block I's products over K < I into chunks of
+// MF_F1_CHUNK tiles (the root's last row would stream 37 tiles through one
+// CTA): chunk 0 stores y_I's gathered entries minus its products in vec2,
+// chunks 1.. store their products as partial sums, and readers of y
+// subtract those in chunk order.
+constexpr int MF_F1_CHUNK = 8;
+__host__ __device__ __forceinline__ int mf_f1_chunks(int I) {
+    return I <= MF_F1_CHUNK ? 1 : (I + MF_F1_CHUNK - 1) / MF_F1_CHUNK;
+}
+// F1 tasks of a front: sum over I < Kt of mf_f1_chunks(I), i.e. 1 (I = 0)
+// plus sum_{I=1}^{n} ceil(I / 8), n = Kt - 1
+__host__ __device__ __forceinline__ int mf_f1_tasks(int Kt) {
+    if (Kt <= 0) return 0;
+    const int n = Kt - 1, q = n / MF_F1_CHUNK, r = n % MF_F1_CHUNK;
+    return 1 + MF_F1_CHUNK * q * (q + 1) / 2 + r * (q + 1);
+}
+// partial-sum slots per pivot row block (the chunks after the first)
+__host__ __device__ __forceinline__ int mf_f1_slots(int Kt) {
+    return Kt >= 2 ? mf_f1_chunks(Kt - 1) - 1 : 0;
+}
+// offset of pivot row block I's F1 partial ch (>= 1) in V.part: after the
+// front's ring partials
+__device__ __forceinline__ long long mf_f1_part(const MfFront &f, int I, int ch) {
+    return f.poff + (long long)f.Kt * mf_ring_chunks(f.Mt - f.Kt) * 64 +
+           ((long long)I * mf_f1_slots(f.Kt) + ch - 1) * 64;
+}
+// element c of y_K
+__device__ __forceinline__ double mf_inv_y(const MfView &V, const MfFront &f, int K, int c) {
+    double y = __ldcg(&V.vec2[f.vec_off + K * 64 + c]);
+    const int nc = mf_f1_chunks(K);
+    for (int ch = 1; ch < nc; ch++) y -= __ldcg(&V.part[mf_f1_part(f, K, ch) + c]);
+    return y;
 }
 
 // Per-thread quarter sums of sum_{i<n} sign(i) T_i x_i: tile(i) points to
@@ -1333,22 +1367,32 @@ __device__ double mf_row_tiles(MfSolveSmem &S, uint32_t *uses, int n, Tile tile,
     return acc;
 }
 
-// F1: pivot row block I of front f.
+// F1 task u of front f: chunk ch of pivot row block I (tiles K in
+// [8 ch, min(I, 8 ch + 8))).
 template <class T>
-__device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, int I,
+__device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, int u,
                           MfSolveSmem &S, uint32_t *uses, int *err) {
+    int I = 0;
+    while (u >= mf_f1_chunks(I)) u -= mf_f1_chunks(I++);
+    const int ch = u, k0 = ch * MF_F1_CHUNK, n = min(I, k0 + MF_F1_CHUNK) - k0;
     const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
     MfFront C0, C1;
     if (h0) C0 = V.fr[f.c0];
     if (h1) C1 = V.fr[f.c1];
     double g = 0.0;
-    if (threadIdx.x < 64) g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
+    if (ch == 0 && threadIdx.x < 64)
+        g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
     const double acc = mf_row_tiles<T>(
-        S, uses, I, [&](int K) { return (const T *)ftile<T>(V, f, I, K); },
-        [&](int K, int c) { return mf_gather_elem(V, f, w, K * 64 + c, h0, C0, h1, C1); },
+        S, uses, n, [&](int i) { return (const T *)ftile<T>(V, f, I, k0 + i); },
+        [&](int i, int c) {
+            return mf_gather_elem(V, f, w, (k0 + i) * 64 + c, h0, C0, h1, C1);
+        },
         [](int) { return 1.0; }, err);
     const double t = mf_reduce_rows(S, acc);
-    if (threadIdx.x < 64) __stcg(&V.vec2[f.vec_off + I * 64 + threadIdx.x], g - t);
+    if (threadIdx.x < 64) {
+        if (ch == 0) __stcg(&V.vec2[f.vec_off + I * 64 + threadIdx.x], g - t);
+        else __stcg(&V.part[mf_f1_part(f, I, ch) + threadIdx.x], t);
+    }
 }
 
 // F2: update row block I (>= Kt) of front f.
@@ -1361,10 +1405,9 @@ __device__ void mf_inv_f2(const MfView &V, const MfFront &f, const double *w, in
     if (h1) C1 = V.fr[f.c1];
     double g = 0.0;
     if (threadIdx.x < 64) g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
-    const double *y = V.vec2 + f.vec_off;
     const double acc = mf_row_tiles<T>(
         S, uses, f.Kt, [&](int K) { return (const T *)ftile<T>(V, f, I, K); },
-        [&](int K, int c) { return __ldcg(&y[K * 64 + c]); }, [](int) { return 1.0; }, err);
+        [&](int K, int c) { return mf_inv_y(V, f, K, c); }, [](int) { return 1.0; }, err);
     const double t = mf_reduce_rows(S, acc);
     if (threadIdx.x < 64) __stcg(&V.vec[f.vec_off + I * 64 + threadIdx.x], g - t);
 }
@@ -1393,13 +1436,12 @@ template <class T>
 __device__ void mf_inv_b2(const MfView &V, const MfFront &f, double *w, int K, MfSolveSmem &S,
                           uint32_t *uses, int *err) {
     const int nch = mf_ring_chunks(f.Mt - f.Kt);
-    const double *y = V.vec2 + f.vec_off;
     const int *var = V.vars + f.var_off;
     const double acc = mf_row_tiles<T>(
         S, uses, f.Kt - K, [&](int i) { return (const T *)ftile<T>(V, f, K, K + i); },
         [&](int i, int c) {
             const int J = K + i;
-            double t = __ldcg(&y[J * 64 + c]);
+            double t = mf_inv_y(V, f, J, c);
             if (nch > 0) {
                 const double *pp = V.part + f.poff + (long long)J * nch * 64 + c;
                 for (int ch = 0; ch < nch; ch++) t -= __ldcg(&pp[ch * 64]);
@@ -1451,8 +1493,8 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
             }
         } else if (V.inv) {
             mf_for_tasks(
-                V, fb, fe, S.km, [](int Kt, int) { return Kt; },
-                [&](const MfFront &f, int I) { mf_inv_f1<T>(V, f, w, I, S, uses, err); });
+                V, fb, fe, S.km, [](int Kt, int) { return mf_f1_tasks(Kt); },
+                [&](const MfFront &f, int u) { mf_inv_f1<T>(V, f, w, u, S, uses, err); });
             grid_barrier(bar, err);
             mf_for_tasks(
                 V, fb, fe, S.km, [](int Kt, int Mt) { return Mt - Kt; },
@@ -1636,7 +1678,7 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
     std::vector<int> cols(rows * sys.ell);
     int rc = check_cuda(s, cudaMemcpyAsync(cols.data(), sys.ell_cols, cols.size() * 4,
                                            cudaMemcpyDeviceToHost, s->stream), "mf pattern");
-    if (!rc) rc = check_cuda(s, cudaStreamSynchronize(s->stream), "mf pattern");
+    if (!rc) rc = stream_sync(s, "mf pattern");
     if (rc) return rc;
     MfPlan &P = D->plan;
     if (!mf_analyse(P, dofs, s->g.Ny1, s->g.Nx1, mf_leaf(s, dofs)) || P.n != sys.n) {
@@ -1670,10 +1712,10 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
         if (modes[p] & MF_SOLVE_LOCAL) continue;
         for (int fi = P.level_begin[p]; fi < P.level_begin[p + 1]; fi++) {
             MfFront &F = P.fronts[fi];
-            const int nch = mf_ring_chunks(F.Mt - F.Kt);
-            if (nch > 0 && F.Kt > 0) {
+            const int slots = mf_ring_chunks(F.Mt - F.Kt) + mf_f1_slots(F.Kt);
+            if (slots > 0 && F.Kt > 0) {   // ring partials, then F1 partials
                 F.poff = poff;
-                poff += (long long)F.Kt * nch * 64;
+                poff += (long long)F.Kt * slots * 64;
             }
             if (F.Kt >= 2) {
                 inv.push_back(make_int2(fi, F.Kt));
@@ -1702,7 +1744,7 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
         s->last_error = std::string("multifrontal allocation: ") + cudaGetErrorString(e);
         return EREBUS_ENOMEM;
     }
-    return check_cuda(s, cudaStreamSynchronize(s->stream), "mf upload");
+    return stream_sync(s, "mf upload");
 }
 
 static int mf_blocks(erebus_state *s, const void *func, size_t smem) {

@@ -108,6 +108,7 @@ struct BandSystem {
     int kdim = 0;                  // restart length the basis below was allocated for
     double *kbasis = nullptr;      // V (kdim + 1 vectors) then Z (kdim vectors), np each
     double *kwork = nullptr;       // dot partials, h, y (device)
+    double *khost = nullptr;       // Hessenberg column and update coefficients (page-locked)
 };
 
 }  // namespace erebus
@@ -122,6 +123,7 @@ struct erebus_state {
     cudaStream_t stream = nullptr;
     int device = 0;
     int64_t launches = 0;
+    int64_t host_syncs = 0;                    // host waits on the state's streams
     // the Stokes-Darcy post-processing sequence as a CUDA graph (stencils.cu),
     // for the solution vector it was captured with
     cudaGraphExec_t post_graph = nullptr;
@@ -186,6 +188,8 @@ struct erebus_state {
 namespace erebus {
 // Launch bookkeeping and error capture.
 int check_cuda(erebus_state *s, cudaError_t e, const char *what);
+// Waits for the state's stream (counted in erebus_state::host_syncs).
+int stream_sync(erebus_state *s, const char *what);
 #define EREBUS_LAUNCH(s, kernel, grid, block, smem, ...)                      \
     do {                                                                      \
         kernel<<<(grid), (block), (smem), (s)->stream>>>(__VA_ARGS__);        \

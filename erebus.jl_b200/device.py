@@ -28,7 +28,8 @@ EXPORTS = [
     "erebus_markers_to_nodes", "erebus_gravity", "erebus_thermochemical_reaction",
     "erebus_hydromech_pass", "erebus_thermal_solve", "erebus_nodes_to_markers",
     "erebus_advect_rk4", "erebus_replenish", "erebus_step", "erebus_export_hydromech",
-    "erebus_apply_hydromech", "erebus_kernel_launches", "erebus_factor_stats",
+    "erebus_apply_hydromech", "erebus_kernel_launches", "erebus_host_syncs",
+    "erebus_factor_stats",
     "erebus_snapshot_begin", "erebus_snapshot_wait", "erebus_adjoint_heat",
     "erebus_step_host", "erebus_share_solver_stream",
 ]
@@ -95,6 +96,7 @@ def load_library(path=LIB_PATH):
         "erebus_export_hydromech": [P, D, pI64, P, P, P, P],
         "erebus_apply_hydromech": [P, D, P, P],
         "erebus_kernel_launches": [P, pI64],
+        "erebus_host_syncs": [P, pI64],
         "erebus_get_stream": [P, PP],
         "erebus_enable_phase_timing": [P, I32],
         "erebus_phase_times": [P, pD, pI64, I32],
@@ -333,6 +335,12 @@ class Simulation:
         n = ctypes.c_int64()
         self._check("erebus_kernel_launches",
                     self.L.erebus_kernel_launches(self.h, ctypes.byref(n)))
+        return n.value
+
+    def host_syncs(self):
+        """Host waits on this state's streams since creation."""
+        n = ctypes.c_int64()
+        self._check("erebus_host_syncs", self.L.erebus_host_syncs(self.h, ctypes.byref(n)))
         return n.value
 
     PHASES = ["markers_to_nodes", "gravity", "reaction", "hydro_assemble", "hydro_factor",

@@ -365,6 +365,13 @@ function kernel_launches(s::State)
     return n[]
 end
 
+function host_syncs(s::State)
+    n = Ref{Int64}(0)
+    check("erebus_host_syncs", s, ccall((:erebus_host_syncs, liberebus), Cint,
+                                        (Ptr{Cvoid}, Ptr{Int64}), s.ptr, n))
+    return n[]
+end
+
 function get_stream(s::State)
     st = Ref{Ptr{Cvoid}}(C_NULL)
     check("erebus_get_stream", s, ccall((:erebus_get_stream, liberebus), Cint,

@@ -420,6 +420,11 @@ int erebus_apply_hydromech(erebus_state *s, double dt, const double *x,
                            double *y);
 /* Number of kernel launches issued by this state since creation. */
 int erebus_kernel_launches(const erebus_state *s, int64_t *count);
+/* Number of times the host waited for this state's streams since creation
+   (a timestep waits where the reference makes a decision: convergence of a
+   solve or of the plastic and thermochemical iterations, the dt updates,
+   the new marker count).  No reference counterpart. */
+int erebus_host_syncs(const erebus_state *s, int64_t *count);
 /* The CUDA stream (cudaStream_t) all work of this state is enqueued on,
    for callers that time it with their own events.  No reference
    counterpart. */

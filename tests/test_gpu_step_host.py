@@ -51,3 +51,18 @@ def test_step_host_rejects_bad_marker_types(pkg, built_lib):
     st.m["tm"][5] = 1
     sim.step_host(1)                            # the state is still usable
     sim.close()
+
+
+def test_host_syncs_are_counted(pkg, built_lib):
+    """erebus_host_syncs counts the host's waits on the state's streams: a
+    timestep waits where the reference decides (solve and iteration
+    convergence, dt, the marker count), a few dozen times, not per kernel."""
+    st = pkg.make_state("planetesimal_41")
+    sim = pkg.Simulation(st)
+    sim.step(1)
+    y0, l0 = sim.host_syncs(), sim.kernel_launches()
+    sim.step(2)
+    dy, dl = sim.host_syncs() - y0, sim.kernel_launches() - l0
+    sim.close()
+    assert 0 < dy < dl, (dy, dl)
+    assert dy < 200, dy
