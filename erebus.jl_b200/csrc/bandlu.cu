@@ -428,7 +428,21 @@ __global__ void k_norms2_part(const double *a, const double *b, int64_t n, doubl
     int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
     int64_t lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
     double xa = 0.0, xb = 0.0;
-    for (int64_t k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+    const int64_t st = blockDim.x;
+    int64_t k = lo + threadIdx.x;
+    for (; k + 3 * st < hi; k += 4 * st) {   // loads in flight first, sums in order
+        const double a0 = a[k], a1 = a[k + st], a2 = a[k + 2 * st], a3 = a[k + 3 * st];
+        const double b0 = b[k], b1 = b[k + st], b2 = b[k + 2 * st], b3 = b[k + 3 * st];
+        xa = fma(a0, a0, xa);
+        xb = fma(b0, b0, xb);
+        xa = fma(a1, a1, xa);
+        xb = fma(b1, b1, xb);
+        xa = fma(a2, a2, xa);
+        xb = fma(b2, b2, xb);
+        xa = fma(a3, a3, xa);
+        xb = fma(b3, b3, xb);
+    }
+    for (; k < hi; k += st) {
         xa = fma(a[k], a[k], xa);
         xb = fma(b[k], b[k], xb);
     }

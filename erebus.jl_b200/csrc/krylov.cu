@@ -55,7 +55,18 @@ __global__ void __launch_bounds__(KT) k_mdot_part(const double *__restrict__ V, 
     for (int i = 0; i < nv; i++) {
         const double *v = V + (int64_t)i * ld;
         double acc = 0.0;
-        for (int64_t k = lo + threadIdx.x; k < hi; k += KT) acc = fma(v[k], w[k], acc);
+        // four elements' loads in flight before their multiply-adds, which
+        // keep the lane's order k, k + KT, k + 2 KT, ...
+        int64_t k = lo + threadIdx.x;
+        for (; k + 3 * KT < hi; k += 4 * KT) {
+            const double a0 = v[k], a1 = v[k + KT], a2 = v[k + 2 * KT], a3 = v[k + 3 * KT];
+            const double b0 = w[k], b1 = w[k + KT], b2 = w[k + 2 * KT], b3 = w[k + 3 * KT];
+            acc = fma(a0, b0, acc);
+            acc = fma(a1, b1, acc);
+            acc = fma(a2, b2, acc);
+            acc = fma(a3, b3, acc);
+        }
+        for (; k < hi; k += KT) acc = fma(v[k], w[k], acc);
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0) red[warp] = acc;
         __syncthreads();
@@ -94,7 +105,16 @@ __global__ void k_maxpy(double *__restrict__ w, const double *__restrict__ V, in
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     double s = 0.0;
-    for (int i = 0; i < nv; i++) s = fma(c[i], V[(int64_t)i * ld + k], s);
+    int i = 0;
+    for (; i + 3 < nv; i += 4) {   // four loads in flight, summed in order
+        const double v0 = V[(int64_t)i * ld + k], v1 = V[(int64_t)(i + 1) * ld + k];
+        const double v2 = V[(int64_t)(i + 2) * ld + k], v3 = V[(int64_t)(i + 3) * ld + k];
+        s = fma(c[i], v0, s);
+        s = fma(c[i + 1], v1, s);
+        s = fma(c[i + 2], v2, s);
+        s = fma(c[i + 3], v3, s);
+    }
+    for (; i < nv; i++) s = fma(c[i], V[(int64_t)i * ld + k], s);
     w[k] = fma(sign, s, w[k]);
 }
 
