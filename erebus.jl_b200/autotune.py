@@ -63,13 +63,15 @@ def tune(make_state, base_opts=None, steps=4, warmup=3, candidates=None, log=pri
     trials = []
     best_ms = time_config(make_state, {**base, **best}, steps, warmup)
     trials.append((dict(best), best_ms))
+    measured = {tuple(sorted(best.items())): best_ms}
     log("start %s: %.3f ms/timestep" % (best, best_ms))
     for name, values in candidates.items():
         for v in values:
-            if v == best[name]:
-                continue
             trial = dict(best, **{name: v})
+            if tuple(sorted(trial.items())) in measured:   # e.g. the value in force
+                continue
             ms = time_config(make_state, {**base, **trial}, steps, warmup)
+            measured[tuple(sorted(trial.items()))] = ms
             trials.append((trial, ms))
             log("%s=%d: %.3f ms/timestep" % (name, v, ms))
             if ms < best_ms:
