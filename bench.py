@@ -475,7 +475,9 @@ def measure_e2e(pkg, args, mode, world):
     st2 = pkg.make_state(args.workload).pinned()
     sim2 = pkg.Simulation(st2)
     sim2.set_solver_options(**MODES[mode])
-    for ts in range(1, 3):
+    # the same timesteps as the device-resident arm: warm-up on the device,
+    # then args.steps timesteps through erebus_step_host
+    for ts in range(1, args.warmup + 1):
         sim2.step(ts)
     sim2.download()
     h2d = sum(a[: st2.marknum].nbytes for k, a in st2.m.items() if k != "etasolidm_m") + \
@@ -484,11 +486,11 @@ def measure_e2e(pkg, args, mode, world):
         h2d += st2.m["etasolidm_m"][: st2.marknum].nbytes
     stream2 = torch.cuda.ExternalStream(sim2.stream_handle())
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ne2e = max(3, min(args.steps, 10))
+    ne2e = args.steps
     barrier(world)
     torch.cuda.synchronize()
     e2.record(stream2)
-    for ts in range(3, 3 + ne2e):
+    for ts in range(args.warmup + 1, args.warmup + 1 + ne2e):
         sim2.step_host(ts)
     e3.record(stream2)
     torch.cuda.synchronize()
