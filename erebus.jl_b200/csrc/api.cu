@@ -1,7 +1,7 @@
 // api.cu -- the extern "C" boundary of liberebus_b200.so (include/erebus_b200.h)
 // and the host-side timestep driver.
 //
-// The driver follows simulation_loop (src/Erebus.jl:6370-7235): every phase
+// The timestep follows simulation_loop (src/Erebus.jl:6370-7235): every phase
 // is enqueued on the state's stream; the host waits only where the
 // reference makes a decision (plastic and thermochemical convergence, the
 // dt updates, the new marker count).

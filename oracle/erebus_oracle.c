@@ -1,7 +1,7 @@
 /*
  * erebus_oracle.c -- CPU oracle for the Erebus.jl timestep hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker against which the
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle against which the
  * CUDA library is compared, and the timed CPU baseline of bench.py.  Nothing
  * in the product (the erebus.jl_b200 package, its CUDA library) links, loads
  * or calls it.

@@ -9,7 +9,7 @@ a committed fixture (tests/golden/planetesimal_401_steps.npz, made by
 tests/golden/make_planetesimal_401.py from the same seeded initial state):
 every 7th P node of the solution fields and every 64th marker after each
 timestep.  The device runs advance their own state (free-running) and must
-match the fixture after each timestep with the north star's bounds --
+match the fixture after each timestep within the library's parity bounds --
 solution fields to 1e-8 relative L2 over the sample, marker positions to
 1e-10 relative -- with the same thermochemical and plastic iteration counts
 and dt, and every solve's scaled residual at most 1e-10.  The two device
