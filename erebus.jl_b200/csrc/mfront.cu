@@ -581,9 +581,17 @@ __device__ __forceinline__ void mf_slot_wait(MfSolveSmem &S, int sl, uint32_t pa
 // CTA barrier it passes, so the slot is refilled without another one.
 template <bool released = false, class Src, class Use>
 __device__ void mf_stream(MfSolveSmem &S, uint32_t *uses, int n, Src src, Use use, int *err) {
+    mf_stream<released>(S, uses, n, src, use, [](int) {}, err);
+}
+// The same with pre(i) called by all threads before tile i is waited for
+// (after the previous tile's use), so its work overlaps the copies in flight.
+template <bool released = false, class Src, class Use, class Pre>
+__device__ void mf_stream(MfSolveSmem &S, uint32_t *uses, int n, Src src, Use use, Pre pre,
+                          int *err) {
     for (int i = 0; i < n && i < MF_SLOTS; i++) mf_fetch(S, i, src(i));
     for (int i = 0; i < n; i++) {
         const int sl = i % MF_SLOTS;
+        pre(i);
         mf_slot_wait(S, sl, uses[sl] & 1u, err);
         uses[sl]++;
         use(i, (const decltype(src(0)))S.tile[sl]);
@@ -1345,8 +1353,10 @@ __device__ double mf_row_tiles(MfSolveSmem &S, uint32_t *uses, int n, Tile tile,
     double acc = 0.0;
     mf_stream(
         S, uses, n, tile,
-        [&](int i, const T *Tt) {
-            if (i % MF_XG == 0) {   // the previous tile's barrier has passed
+        [&](int i, const T *Tt) { acc += sign(i) * mf_quarter(Tt, S.vs + (i % MF_XG) * 64); },
+        [&](int i) {
+            if (i % MF_XG == 0) {   // staged while the tiles' copies are in flight; the
+                                    // previous tile's barrier has passed
                 const int m = min(n - i, MF_XG) * 64;
                 double v[4];
 #pragma unroll
@@ -1361,7 +1371,6 @@ __device__ double mf_row_tiles(MfSolveSmem &S, uint32_t *uses, int n, Tile tile,
                 }
                 __syncthreads();
             }
-            acc += sign(i) * mf_quarter(Tt, S.vs + (i % MF_XG) * 64);
         },
         err);
     return acc;
