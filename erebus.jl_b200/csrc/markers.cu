@@ -983,6 +983,71 @@ __device__ __forceinline__ double vy_at(const Geo &g, const double *v, double x,
     return (1.0 - dxmj / dx) * v12 + (dxmj / dx) * v34;
 }
 
+// The velocity interpolations of the RK4 advection with the cell fractions
+// taken as products with 1/dx and 1/dy and the blends as fused multiply-adds
+// (the k_backtrace versions above keep the reference's divisions and
+// roundings).  The results differ from those by rounding only (~1e-16
+// relative); the advection is bound by its FP64 instructions, not by HBM.
+struct RkGeo {
+    double dx, dy, idx, idy;
+    int Nx, Ny, Ny1;
+};
+__device__ __forceinline__ void rk_cell(double x, double y, double x0, double y0,
+                                        const RkGeo &r, int jmax_, int imax_, int &i, int &j,
+                                        double &fx, double &fy) {
+    int64_t jj = jtrunc((x - x0) * r.idx) + 1, ii = jtrunc((y - y0) * r.idy) + 1;
+    jj = jj < 1 ? 1 : jj > jmax_ ? jmax_ : jj;
+    ii = ii < 1 ? 1 : ii > imax_ ? imax_ : ii;
+    j = (int)jj;
+    i = (int)ii;
+    fx = (x - ax(x0, r.dx, j)) * r.idx;
+    fy = (y - ax(y0, r.dy, i)) * r.idy;
+}
+__device__ __forceinline__ double rk_vx(const RkGeo &r, const double *__restrict__ v,
+                                        const double *__restrict__ vq, bool quirk, double x,
+                                        double y) {
+    int i, j;
+    double fx, fy;
+    rk_cell(x, y, 0.0, -r.dy / 2, r, r.Nx - 1, r.Ny, i, j, fx, fy);
+    const int Ny1 = r.Ny1;
+    const double a0 = AT(v, Ny1, i, j), a1 = AT(v, Ny1, i, j + 1);
+    const double b0 = AT(v, Ny1, i + 1, j), b1 = AT(v, Ny1, i + 1, j + 1);
+    double v13 = fma(fx, a1 - a0, a0), v24 = fma(fx, b1 - b0, b0);
+    const double q = fx - 0.5, h = 0.5 * (q * q);
+    if (fx >= 0.5) {
+        if (j < r.Nx - 1) {
+            v13 = fma(h, a0 - 2.0 * a1 + AT(v, Ny1, i, j + 2), v13);
+            v24 = fma(h, b0 - 2.0 * b1 + AT(v, Ny1, i + 1, j + 2), v24);
+        }
+    } else if (j > 1) {
+        const double c0 = quirk ? AT(vq, Ny1, i, j) : a0;
+        v13 = fma(h, AT(v, Ny1, i, j - 1) - 2.0 * c0 + a1, v13);
+        v24 = fma(h, AT(v, Ny1, i + 1, j - 1) - 2.0 * b0 + b1, v24);
+    }
+    return fma(fy, v24 - v13, v13);
+}
+__device__ __forceinline__ double rk_vy(const RkGeo &r, const double *__restrict__ v, double x,
+                                        double y) {
+    int i, j;
+    double fx, fy;
+    rk_cell(x, y, -r.dx / 2, 0.0, r, r.Nx, r.Ny - 1, i, j, fx, fy);
+    const int Ny1 = r.Ny1;
+    const double a0 = AT(v, Ny1, i, j), a1 = AT(v, Ny1, i + 1, j);
+    const double b0 = AT(v, Ny1, i, j + 1), b1 = AT(v, Ny1, i + 1, j + 1);
+    double v12 = fma(fy, a1 - a0, a0), v34 = fma(fy, b1 - b0, b0);
+    const double q = fy - 0.5, h = 0.5 * (q * q);
+    if (fy >= 0.5) {
+        if (i < r.Ny - 1) {
+            v12 = fma(h, a0 - 2.0 * a1 + AT(v, Ny1, i + 2, j), v12);
+            v34 = fma(h, b0 - 2.0 * b1 + AT(v, Ny1, i + 2, j + 1), v34);
+        }
+    } else if (i > 1) {
+        v12 = fma(h, AT(v, Ny1, i - 1, j) - 2.0 * a0 + a1, v12);
+        v34 = fma(h, AT(v, Ny1, i - 1, j + 1) - 2.0 * b0 + b1, v34);
+    }
+    return fma(fx, v34 - v12, v12);
+}
+
 // 7 blocks of 128 threads per SM (72 registers a thread, against 84 and 6
 // blocks unbounded): the kernel is bound by the latency of its FP64
 // divisions and gathers, so it wants warps in flight more than registers.
@@ -1007,11 +1072,12 @@ k_rk4(ErebusParams p, Geo g, MP M, GPtr G, int n, double dt) {
     M.f[M_sxxm][m] = sxx * (c * c) - sxx * (sn * sn) - sxy * s2;
     M.f[M_sxym][m] = sxx * s2 + sxy * c2;
     const double *vx = G.f[G_vx], *vy = G.f[G_vy], *vxf = G.f[G_vxf], *vyf = G.f[G_vyf];
+    const RkGeo r = {g.dx, g.dy, 1.0 / g.dx, 1.0 / g.dy, g.Nx, g.Ny, g.Ny1};
     double vxr[4], vyr[4], xr = xmm, yr = ymm;
 #pragma unroll
     for (int rk = 0; rk < 4; rk++) {
-        vxr[rk] = 0.0 + vx_at(g, vx, vx, false, xr, yr, 0);
-        vyr[rk] = 0.0 + vy_at(g, vy, xr, yr, 0);
+        vxr[rk] = rk_vx(r, vx, vx, false, xr, yr);
+        vyr[rk] = rk_vy(r, vy, xr, yr);
         if (rk < 3) {
             xr = xmm + dt * Cc[rk] * vxr[rk];
             yr = ymm + dt * Cc[rk] * vyr[rk];
@@ -1025,8 +1091,8 @@ k_rk4(ErebusParams p, Geo g, MP M, GPtr G, int n, double dt) {
     ymm = yr = yn;
 #pragma unroll
     for (int rk = 0; rk < 4; rk++) {
-        vxr[rk] = 0.0 + vx_at(g, vxf, vx, true, xr, yr, 0);
-        vyr[rk] = 0.0 + vy_at(g, vyf, xr, yr, 0);
+        vxr[rk] = rk_vx(r, vxf, vx, true, xr, yr);
+        vyr[rk] = rk_vy(r, vyf, xr, yr);
         if (rk < 3) {
             xr = xmm - dt * Cc[rk] * vxr[rk];
             yr = ymm - dt * Cc[rk] * vyr[rk];
