@@ -600,6 +600,7 @@ int mf_check_error(erebus_state *s, BandSystem &sys, const char *what) {
                          : h == 3 ? ": wait timed out"
                                   : ": matrix pattern changed since the analysis");
         cudaMemsetAsync(sys.err, 0, sizeof(int), s->stream);
+        mf_clear_counts(s, sys);
         if (h == 4) mf_release(sys);   // analysed again at the next factorisation
         return h == 2 ? EREBUS_ENOCONV : EREBUS_ECUDA;
     }

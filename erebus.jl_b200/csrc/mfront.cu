@@ -46,7 +46,7 @@ struct MfView {
     const int *eamap;   // local -> children's update index
     const int *lvl;     // level ranges (nlev + 1)
     const int *lvl_kt;  // max Kt per level
-    const int *lvl_mode;  // per level: MF_FACTOR_LOCAL, MF_SOLVE_LOCAL bits
+    const int *lvl_mode;  // per level: MF_FACTOR_LOCAL, MF_SOLVE_LOCAL, ... bits
     int *flags;         // per 64-row block of the front vectors: the solve epoch it is final in
     double *vec2;       // pivot part of the forward solution (levels with inverted pivot blocks)
     double *part;       // partial sums of the backward ring products (MfFront::poff)
@@ -247,6 +247,11 @@ constexpr int MF_FACTOR_LOCAL = 1, MF_SOLVE_LOCAL = 2;
 // (M <= MF_VS_MAX), so the level's sweeps stream all of a CTA's fronts
 // through one tile pipeline.
 constexpr int MF_SOLVE_VS = 4;
+// Cooperative solve levels whose update rows (F2) or pivot rows (B2) run in
+// 8-tile chunks: set where a front has rows of more than 12 tiles and the
+// chunked tasks of the phase still fit one wave of the grid (more tasks per
+// CTA cost more than the shorter rows save).
+constexpr int MF_CHUNK_F2 = 8, MF_CHUNK_B2 = 16;
 
 struct MfFactorSmem {
     MmaSmem m;
@@ -512,6 +517,17 @@ constexpr int MF_SLOTS = 3;
 // one CTA barrier and no round trip to L2.
 constexpr int MF_VS_MAX = 1024;
 
+// What the one-front-per-CTA sweeps read of a front's descriptor.  A CTA
+// loads the records of up to MF_LF_MAX of its fronts of a level at once (one
+// thread per front, its children's descriptors too) instead of each front's
+// descriptor, then its children's, when the front starts.
+struct MfLf {
+    long long off, var_off, map_off, vec_off;
+    long long c0v, c1v;   // children's update parts in V.vec (-1: no child)
+    int M, Kp, k, Kt, Mt, pad;
+};
+constexpr int MF_LF_MAX = MF_KM_MAX * (int)sizeof(int2) / (int)sizeof(MfLf);
+
 struct MfSolveSmem {
     double tile[MF_SLOTS][T2];
     unsigned long long bar[MF_SLOTS];
@@ -519,7 +535,11 @@ struct MfSolveSmem {
     double x[64];          // vector piece the current tile multiplies
     double y[64];
     double vs[MF_VS_MAX];  // the front vector of a front swept by one CTA
-    int2 km[MF_KM_MAX];    // (Kt, Mt) of the level's fronts
+    union {
+        int2 km[MF_KM_MAX];   // cooperative levels: (Kt, Mt) of the level's fronts
+        MfLf lf[MF_LF_MAX];   // one-front-per-CTA levels: a batch of this CTA's fronts
+    };
+    int last;              // this CTA's chunk of a row arrived last
 };
 // two CTAs per SM
 static_assert(sizeof(MfSolveSmem) <= 113 * 1024, "solve shared memory");
@@ -930,17 +950,64 @@ __device__ void mf_bwd_front_s(const MfView &V, const MfFront &f, double *w, MfS
 // tiles are in flight while the current front finishes and the next one is
 // gathered.
 
+// Records of this CTA's fronts fi, fi + G, ... (at most MF_LF_MAX, below
+// fe) into lf; `children` adds the children's update-part offsets.  Called
+// by all threads; ends with a barrier.
+template <bool children>
+__device__ void mf_load_lf(const MfView &V, int fi, int G, int fe, MfLf *lf) {
+    const int q = threadIdx.x, f_i = fi + q * G;
+    if (q < MF_LF_MAX && f_i < fe) {
+        const MfFront f = V.fr[f_i];
+        MfLf r;
+        r.off = f.off;
+        r.var_off = f.var_off;
+        r.map_off = f.map_off;
+        r.vec_off = f.vec_off;
+        r.M = f.M;
+        r.Kp = f.Kp;
+        r.k = f.k;
+        r.Kt = f.Kt;
+        r.Mt = f.Mt;
+        r.pad = 0;
+        r.c0v = r.c1v = -1;
+        if (children) {
+            if (f.c0 >= 0) r.c0v = V.fr[f.c0].vec_off + V.fr[f.c0].Kp;
+            if (f.c1 >= 0) r.c1v = V.fr[f.c1].vec_off + V.fr[f.c1].Kp;
+        }
+        lf[q] = r;
+    }
+    __syncthreads();
+}
+
+// (off, Kt, Mt) of front fi for a fetch cursor (thread 0): from the batch
+// of records in lf that starts at front lf0 when fi is in it, else from the
+// descriptor in global memory.
+__device__ __forceinline__ void mf_cursor_front(const MfView &V, const MfLf *lf, int lf0,
+                                                int lfn, int G, int fi, long long &off,
+                                                int &Kt, int &Mt) {
+    const int q = (fi - lf0) / G;
+    if (fi >= lf0 && q < lfn) {
+        off = lf[q].off;
+        Kt = lf[q].Kt;
+        Mt = lf[q].Mt;
+    } else {
+        const MfFront &F = V.fr[fi];
+        off = F.off;
+        Kt = F.Kt;
+        Mt = F.Mt;
+    }
+}
+
 // Fetch cursor of the forward sweep: tiles (I, K), K < Kt, I = K+1..Mt-1.
 template <class T>
 struct MfFwdCursor {
     int fi, fe, G, K, I, Kt, Mt;
     long long off;
+    const MfLf *lf;
+    int lf0, lfn;   // the batch of records in lf: fronts lf0, lf0 + G, ... (lfn of them)
     __device__ void load(const MfView &V) {
         if (fi < fe) {
-            const MfFront &F = V.fr[fi];
-            off = F.off;
-            Kt = F.Kt;
-            Mt = F.Mt;
+            mf_cursor_front(V, lf, lf0, lfn, G, fi, off, Kt, Mt);
             K = 0;
             I = 1;
         }
@@ -965,12 +1032,11 @@ template <class T>
 struct MfBwdCursor {
     int fi, fe, G, K, j, ring, Kt, Mt;
     long long off;
+    const MfLf *lf;
+    int lf0, lfn;   // as in MfFwdCursor
     __device__ void load(const MfView &V) {
         if (fi < fe) {
-            const MfFront &F = V.fr[fi];
-            off = F.off;
-            Kt = F.Kt;
-            Mt = F.Mt;
+            mf_cursor_front(V, lf, lf0, lfn, G, fi, off, Kt, Mt);
             ring = Mt > Kt;
             K = ring ? 0 : Kt - 1;
             j = 0;
@@ -1014,11 +1080,16 @@ __device__ void mf_fwd_level_s(const MfView &V, int fb, int fe, const double *w,
     constexpr int NS = MfSlots<T>::n;
     const int G = gridDim.x;
     double *vs = S.vs;
+    const int fi0 = fb + blockIdx.x;
+    mf_load_lf<true>(V, fi0, G, fe, S.lf);
     MfFwdCursor<T> cur;
     if (threadIdx.x == 0) {
-        cur.fi = fb + blockIdx.x;
+        cur.fi = fi0;
         cur.fe = fe;
         cur.G = G;
+        cur.lf = S.lf;
+        cur.lf0 = fi0;
+        cur.lfn = MF_LF_MAX;
         cur.load(V);
         for (int q = 0; q < NS; q++) {
             const T *p = cur.next(V);
@@ -1026,25 +1097,27 @@ __device__ void mf_fwd_level_s(const MfView &V, int fb, int fe, const double *w,
             mf_fetch(S, q, p);
         }
     }
-    int sl = 0;
-    for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
-        const MfFront f = V.fr[fi];
+    int sl = 0, q = 0;
+    for (int fi = fi0; fi < fe; fi += G, q++) {
+        if (q == MF_LF_MAX) {   // every thread is past the batch's last front
+            q = 0;
+            mf_load_lf<true>(V, fi, G, fe, S.lf);
+            if (threadIdx.x == 0) cur.lf0 = fi;
+        }
+        const MfLf &f = S.lf[q];
         {
             const int *var = V.vars + f.var_off, *map = V.eamap + f.map_off;
-            MfFront C0, C1;
-            const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
-            if (h0) C0 = V.fr[f.c0];
-            if (h1) C1 = V.fr[f.c1];
+            const long long c0v = f.c0v, c1v = f.c1v;
             for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
                 int g = var[a];
                 double s = (a < f.Kp && g >= 0) ? __ldcg(&w[g]) : 0.0;
-                if (h0) {
+                if (c0v >= 0) {
                     int i = map[2 * a];
-                    if (i >= 0) s += __ldcg(&V.vec[C0.vec_off + C0.Kp + i]);
+                    if (i >= 0) s += __ldcg(&V.vec[c0v + i]);
                 }
-                if (h1) {
+                if (c1v >= 0) {
                     int i = map[2 * a + 1];
-                    if (i >= 0) s += __ldcg(&V.vec[C1.vec_off + C1.Kp + i]);
+                    if (i >= 0) s += __ldcg(&V.vec[c1v + i]);
                 }
                 vs[a] = s;
             }
@@ -1084,11 +1157,16 @@ __device__ void mf_bwd_level_s(const MfView &V, int fb, int fe, double *w, MfSol
     constexpr int NS = MfSlots<T>::n;
     const int G = gridDim.x;
     double *vs = S.vs;
+    const int fi0 = fb + blockIdx.x;
+    mf_load_lf<false>(V, fi0, G, fe, S.lf);
     MfBwdCursor<T> cur;
     if (threadIdx.x == 0) {
-        cur.fi = fb + blockIdx.x;
+        cur.fi = fi0;
         cur.fe = fe;
         cur.G = G;
+        cur.lf = S.lf;
+        cur.lf0 = fi0;
+        cur.lfn = MF_LF_MAX;
         cur.load(V);
         for (int q = 0; q < NS; q++) {
             const T *p = cur.next(V);
@@ -1104,8 +1182,14 @@ __device__ void mf_bwd_level_s(const MfView &V, int fb, int fe, double *w, MfSol
         }
         sl = sl + 1 == NS ? 0 : sl + 1;
     };
-    for (int fi = fb + blockIdx.x; fi < fe; fi += G) {
-        const MfFront f = V.fr[fi];
+    int q = 0;
+    for (int fi = fi0; fi < fe; fi += G, q++) {
+        if (q == MF_LF_MAX) {   // every thread is past the batch's last front
+            q = 0;
+            mf_load_lf<false>(V, fi, G, fe, S.lf);
+            if (threadIdx.x == 0) cur.lf0 = fi;
+        }
+        const MfLf &f = S.lf[q];
         double *v = V.vec + f.vec_off;
         const int *var = V.vars + f.var_off;
         for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
@@ -1344,13 +1428,63 @@ __device__ __forceinline__ double mf_inv_y(const MfView &V, const MfFront &f, in
     return y;
 }
 
+// Update rows (F2, Kt tiles each) and pivot rows (B2, Kt - K tiles) of more
+// than MF_F1_CHUNK tiles are split into chunks of MF_F1_CHUNK tiles, each a
+// task of its own (the root's first pivot row would stream 38 tiles through
+// one CTA).  Every chunk stores its partial row product; the chunk that
+// arrives last (a count per row block, in V.flags, which the inverted form
+// does not otherwise use) adds the partials in chunk order and writes the
+// row, so the result does not depend on which CTA finishes last.
+__host__ __device__ __forceinline__ int mf_row_chunks(int n) {
+    return n <= MF_F1_CHUNK ? 1 : (n + MF_F1_CHUNK - 1) / MF_F1_CHUNK;
+}
+// B2 tasks of a front: sum over K < Kt of mf_row_chunks(Kt - K), i.e.
+// sum_{m=1}^{Kt} ceil(m / 8)
+__host__ __device__ __forceinline__ int mf_b2_tasks(int Kt) {
+    if (Kt <= 0) return 0;
+    const int q = Kt / MF_F1_CHUNK, r = Kt % MF_F1_CHUNK;
+    return MF_F1_CHUNK * q * (q + 1) / 2 + r * (q + 1);
+}
+// partial-sum slots of a front's chunked rows: chunks of every row block
+__host__ __device__ __forceinline__ long long mf_row_slots(int Kt, int Mt) {
+    return Kt > MF_F1_CHUNK ? (long long)Mt * mf_row_chunks(Kt) : 0;
+}
+// offset of chunk ch of row block I's partial in V.part: after the ring and
+// F1 partials
+__device__ __forceinline__ long long mf_row_part(const MfFront &f, int I, int ch) {
+    return f.poff +
+           (long long)f.Kt * (mf_ring_chunks(f.Mt - f.Kt) + mf_f1_slots(f.Kt)) * 64 +
+           ((long long)I * mf_row_chunks(f.Kt) + ch) * 64;
+}
+// Called by all threads after threads 0..63 stored their chunk's partial:
+// counts the chunk in *cnt and returns, in every thread, whether it was the
+// last of the row's nch.  The last one resets the count for the next solve
+// and may then read the other chunks' partials through L2.
+__device__ __forceinline__ bool mf_chunk_arrive(int *cnt, int nch, MfSolveSmem &S) {
+    __threadfence();   // this thread's partial before the count
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const bool last = atomicAdd(cnt, 1) + 1 == nch;
+        if (last) {
+            atomicExch(cnt, 0);
+            __threadfence();
+        }
+        S.last = last;
+    }
+    __syncthreads();
+    return S.last;
+}
+
 // Per-thread quarter sums of sum_{i<n} sign(i) T_i x_i: tile(i) points to
 // T_i, piece(i, c) gives element c of x_i; the pieces are staged in
-// S.vs MF_XG at a time while the tiles stream.
-template <class T, class Tile, class Piece, class Sign>
+// S.vs MF_XG at a time while the tiles stream.  first() runs in all threads
+// once, after the first tiles' copies and the first pieces' loads are
+// issued, so the task's own gather overlaps both.
+template <class T, class Tile, class Piece, class Sign, class First>
 __device__ double mf_row_tiles(MfSolveSmem &S, uint32_t *uses, int n, Tile tile, Piece piece,
-                               Sign sign, int *err) {
+                               Sign sign, First first, int *err) {
     double acc = 0.0;
+    if (n == 0) first();
     mf_stream(
         S, uses, n, tile,
         [&](int i, const T *Tt) { acc += sign(i) * mf_quarter(Tt, S.vs + (i % MF_XG) * 64); },
@@ -1364,6 +1498,7 @@ __device__ double mf_row_tiles(MfSolveSmem &S, uint32_t *uses, int n, Tile tile,
                     const int e = threadIdx.x + q * LU_THREADS;
                     v[q] = e < m ? piece(i + (e >> 6), e & 63) : 0.0;
                 }
+                if (i == 0) first();
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const int e = threadIdx.x + q * LU_THREADS;
@@ -1389,14 +1524,17 @@ __device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, in
     if (h0) C0 = V.fr[f.c0];
     if (h1) C1 = V.fr[f.c1];
     double g = 0.0;
-    if (ch == 0 && threadIdx.x < 64)
-        g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
     const double acc = mf_row_tiles<T>(
         S, uses, n, [&](int i) { return (const T *)ftile<T>(V, f, I, k0 + i); },
         [&](int i, int c) {
             return mf_gather_elem(V, f, w, (k0 + i) * 64 + c, h0, C0, h1, C1);
         },
-        [](int) { return 1.0; }, err);
+        [](int) { return 1.0; },
+        [&]() {
+            if (ch == 0 && threadIdx.x < 64)
+                g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
+        },
+        err);
     const double t = mf_reduce_rows(S, acc);
     if (threadIdx.x < 64) {
         if (ch == 0) __stcg(&V.vec2[f.vec_off + I * 64 + threadIdx.x], g - t);
@@ -1404,21 +1542,42 @@ __device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, in
     }
 }
 
-// F2: update row block I (>= Kt) of front f.
+// F2: chunk ch of nrc of update row block I (>= Kt) of front f, tiles K in
+// [8 ch, 8 ch + 8) (all Kt when nrc = 1): v_I = gathered entries
+// minus sum_K L_IK y_K.  Chunk 0's partial holds the gathered entries minus
+// its products, the later ones their products.
 template <class T>
-__device__ void mf_inv_f2(const MfView &V, const MfFront &f, const double *w, int I,
-                          MfSolveSmem &S, uint32_t *uses, int *err) {
+__device__ void mf_inv_f2(const MfView &V, const MfFront &f, const double *w, int I, int ch,
+                          int nrc, MfSolveSmem &S, uint32_t *uses, int *err) {
+    const int k0 = ch * MF_F1_CHUNK;
+    const int n = nrc == 1 ? f.Kt : min(MF_F1_CHUNK, f.Kt - k0);
     const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
     MfFront C0, C1;
     if (h0) C0 = V.fr[f.c0];
     if (h1) C1 = V.fr[f.c1];
     double g = 0.0;
-    if (threadIdx.x < 64) g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
     const double acc = mf_row_tiles<T>(
-        S, uses, f.Kt, [&](int K) { return (const T *)ftile<T>(V, f, I, K); },
-        [&](int K, int c) { return mf_inv_y(V, f, K, c); }, [](int) { return 1.0; }, err);
+        S, uses, n, [&](int i) { return (const T *)ftile<T>(V, f, I, k0 + i); },
+        [&](int i, int c) { return mf_inv_y(V, f, k0 + i, c); }, [](int) { return 1.0; },
+        [&]() {
+            if (ch == 0 && threadIdx.x < 64)
+                g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
+        },
+        err);
     const double t = mf_reduce_rows(S, acc);
-    if (threadIdx.x < 64) __stcg(&V.vec[f.vec_off + I * 64 + threadIdx.x], g - t);
+    double *v = V.vec + f.vec_off + I * 64;
+    if (nrc == 1) {
+        if (threadIdx.x < 64) __stcg(&v[threadIdx.x], g - t);
+        return;
+    }
+    if (threadIdx.x < 64)
+        __stcg(&V.part[mf_row_part(f, I, ch) + threadIdx.x], ch == 0 ? g - t : t);
+    if (!mf_chunk_arrive(mf_flag(V, f, I), nrc, S)) return;
+    if (threadIdx.x < 64) {
+        double r = __ldcg(&V.part[mf_row_part(f, I, 0) + threadIdx.x]);
+        for (int c = 1; c < nrc; c++) r -= __ldcg(&V.part[mf_row_part(f, I, c) + threadIdx.x]);
+        __stcg(&v[threadIdx.x], r);
+    }
 }
 
 // B1: ring tiles [Kt + 16 ch, ...) of pivot row block K of front f.
@@ -1434,31 +1593,44 @@ __device__ void mf_inv_b1(const MfView &V, const MfFront &f, const double *w, in
             const int g = var[(j0 + j) * 64 + c];
             return g >= 0 ? __ldcg(&w[g]) : 0.0;
         },
-        [](int) { return 1.0; }, err);
+        [](int) { return 1.0; }, []() {}, err);
     const double t = mf_reduce_rows(S, acc);
     if (threadIdx.x < 64)
         __stcg(&V.part[f.poff + ((long long)K * nch + ch) * 64 + threadIdx.x], t);
 }
 
-// B2: pivot row block K of front f; the solution goes to w.
+// B2: chunk ch of pivot row block K of front f, tiles (K, K + i) for i in
+// [8 ch, 8 ch + 8) (all Kt - K when the row has one chunk or the level is not
+// `chunked`); the solution
+// x_K = D_K^{-1} t_K - sum_{J>K} Z_KJ t_J goes to w.
 template <class T>
-__device__ void mf_inv_b2(const MfView &V, const MfFront &f, double *w, int K, MfSolveSmem &S,
-                          uint32_t *uses, int *err) {
+__device__ void mf_inv_b2(const MfView &V, const MfFront &f, double *w, int K, int ch,
+                          bool chunked, MfSolveSmem &S, uint32_t *uses, int *err) {
     const int nch = mf_ring_chunks(f.Mt - f.Kt);
     const int *var = V.vars + f.var_off;
+    const int m = f.Kt - K, nrc = chunked ? mf_row_chunks(m) : 1, i0 = ch * MF_F1_CHUNK;
+    const int n = nrc == 1 ? m : min(MF_F1_CHUNK, m - i0);
     const double acc = mf_row_tiles<T>(
-        S, uses, f.Kt - K, [&](int i) { return (const T *)ftile<T>(V, f, K, K + i); },
+        S, uses, n, [&](int i) { return (const T *)ftile<T>(V, f, K, K + i0 + i); },
         [&](int i, int c) {
-            const int J = K + i;
+            const int J = K + i0 + i;
             double t = mf_inv_y(V, f, J, c);
             if (nch > 0) {
                 const double *pp = V.part + f.poff + (long long)J * nch * 64 + c;
-                for (int ch = 0; ch < nch; ch++) t -= __ldcg(&pp[ch * 64]);
+                for (int q = 0; q < nch; q++) t -= __ldcg(&pp[q * 64]);
             }
             return t;
         },
-        [](int i) { return i == 0 ? 1.0 : -1.0; }, err);
-    const double x = mf_reduce_rows(S, acc);
+        [=](int i) { return i0 + i == 0 ? 1.0 : -1.0; }, []() {}, err);
+    double x = mf_reduce_rows(S, acc);
+    if (nrc > 1) {
+        if (threadIdx.x < 64) __stcg(&V.part[mf_row_part(f, K, ch) + threadIdx.x], x);
+        if (!mf_chunk_arrive(mf_flag(V, f, K), nrc, S)) return;
+        if (threadIdx.x < 64) {
+            x = __ldcg(&V.part[mf_row_part(f, K, 0) + threadIdx.x]);
+            for (int c = 1; c < nrc; c++) x += __ldcg(&V.part[mf_row_part(f, K, c) + threadIdx.x]);
+        }
+    }
     if (threadIdx.x < 64) {
         const int a = K * 64 + threadIdx.x;
         if (a < f.k) __stcg(&w[var[a]], x);
@@ -1505,9 +1677,14 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
                 V, fb, fe, S.km, [](int Kt, int) { return mf_f1_tasks(Kt); },
                 [&](const MfFront &f, int u) { mf_inv_f1<T>(V, f, w, u, S, uses, err); });
             grid_barrier(bar, err);
+            const bool cf = V.lvl_mode[p] & MF_CHUNK_F2;
             mf_for_tasks(
-                V, fb, fe, S.km, [](int Kt, int Mt) { return Mt - Kt; },
-                [&](const MfFront &f, int u) { mf_inv_f2<T>(V, f, w, f.Kt + u, S, uses, err); });
+                V, fb, fe, S.km,
+                [cf](int Kt, int Mt) { return (Mt - Kt) * (cf ? mf_row_chunks(Kt) : 1); },
+                [&](const MfFront &f, int u) {
+                    const int nrc = cf ? mf_row_chunks(f.Kt) : 1;
+                    mf_inv_f2<T>(V, f, w, f.Kt + u / nrc, u % nrc, nrc, S, uses, err);
+                });
         } else {
             // one task per row block, in increasing order within each front
             mf_for_tasks(
@@ -1550,9 +1727,19 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
                     mf_inv_b1<T>(V, f, w, u / nch, u % nch, S, uses, err);
                 });
             grid_barrier(bar, err);
+            const bool cb = V.lvl_mode[p] & MF_CHUNK_B2;
             mf_for_tasks(
-                V, fb, fe, S.km, [](int Kt, int) { return Kt; },
-                [&](const MfFront &f, int K) { mf_inv_b2<T>(V, f, w, K, S, uses, err); });
+                V, fb, fe, S.km, [cb](int Kt, int) { return cb ? mf_b2_tasks(Kt) : Kt; },
+                [&](const MfFront &f, int u) {
+                    int K = 0;
+                    if (cb) {
+                        while (u >= mf_row_chunks(f.Kt - K)) u -= mf_row_chunks(f.Kt - K++);
+                    } else {
+                        K = u;
+                        u = 0;
+                    }
+                    mf_inv_b2<T>(V, f, w, K, u, cb, S, uses, err);
+                });
         } else {
             // one task per pivot row block, the last first
             mf_for_tasks(
@@ -1591,6 +1778,15 @@ static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
 }
 
 bool mf_is_fp32(const BandSystem &sys) { return sys.mf && sys.mf->fp32; }
+
+// Zeroes the row-block flags (the chunk counts of the inverted form): after
+// a solve that gave up, counts of chunks that never arrived must not carry
+// over into the next solve.
+void mf_clear_counts(erebus_state *s, BandSystem &sys) {
+    MfDevice *D = sys.mf;
+    if (!D || !D->flags) return;
+    cudaMemsetAsync(D->flags, 0, (D->plan.vec / MF_TILE + 1) * sizeof(int), s->stream);
+}
 
 void mf_release(BandSystem &sys) {
     MfDevice *D = sys.mf;
@@ -1662,6 +1858,18 @@ static std::vector<int> mf_level_modes(const MfPlan &P, int G, int factor_ops,
         if (vs) m |= MF_SOLVE_VS;
         if (forced || waves * ops <= factor_ops) m |= MF_FACTOR_LOCAL;
         if (forced || waves * tiles <= solve_tiles) m |= MF_SOLVE_LOCAL;
+        long long f2 = 0, b2 = 0;
+        bool longrows = false;
+        for (int fi = fb; fi < fe; fi++) {
+            const MfFront &f = P.fronts[fi];
+            f2 += (long long)(f.Mt - f.Kt) * mf_row_chunks(f.Kt);
+            b2 += mf_b2_tasks(f.Kt);
+            // a row of 9-12 tiles gains less than a chunk's count and
+            // partial-sum reads cost
+            longrows = longrows || f.Kt > MF_F1_CHUNK + MF_F1_CHUNK / 2;
+        }
+        if (longrows && f2 <= G) m |= MF_CHUNK_F2;
+        if (longrows && b2 <= G) m |= MF_CHUNK_B2;
         mode.push_back(m);
     }
     return mode;
@@ -1721,10 +1929,12 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
         if (modes[p] & MF_SOLVE_LOCAL) continue;
         for (int fi = P.level_begin[p]; fi < P.level_begin[p + 1]; fi++) {
             MfFront &F = P.fronts[fi];
-            const int slots = mf_ring_chunks(F.Mt - F.Kt) + mf_f1_slots(F.Kt);
-            if (slots > 0 && F.Kt > 0) {   // ring partials, then F1 partials
+            const long long slots = (long long)F.Kt * (mf_ring_chunks(F.Mt - F.Kt) +
+                                                       mf_f1_slots(F.Kt)) +
+                                    mf_row_slots(F.Kt, F.Mt);
+            if (slots > 0 && F.Kt > 0) {   // ring partials, F1 partials, chunked rows
                 F.poff = poff;
-                poff += (long long)F.Kt * slots * 64;
+                poff += slots * 64;
             }
             if (F.Kt >= 2) {
                 inv.push_back(make_int2(fi, F.Kt));

@@ -61,6 +61,7 @@ int mf_factor(erebus_state *s, BandSystem &sys, bool fp32);
 bool mf_is_fp32(const BandSystem &sys);
 int mf_solve(erebus_state *s, BandSystem &sys, double *w);
 void mf_release(BandSystem &sys);
+void mf_clear_counts(erebus_state *s, BandSystem &sys);
 void mf_stats(const erebus_state *s, const BandSystem &sys, ErebusFactorStats *o);
 void band_stats(const BandSystem &sys, ErebusFactorStats *o);
 // Residual and norm kernels of the refinement loop (bandlu.cu), shared with

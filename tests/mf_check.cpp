@@ -102,12 +102,20 @@ int solve_inverted(const MfPlan &P, std::vector<double> &S, const double *b, dou
                     for (int r = 0; r < T; r++) y[I * T + r] -= Y[c * T + r] * v[K * T + c];
             }
         }
-        for (int I = F.Kt; I < F.Mt; I++)         // update rows
-            for (int K = 0; K < F.Kt; K++) {
-                const double *L = tile(S, F, I, K);
-                for (int c = 0; c < T; c++)
-                    for (int r = 0; r < T; r++) v[I * T + r] -= L[c * T + r] * y[K * T + c];
+        for (int I = F.Kt; I < F.Mt; I++) {       // update rows, 8-tile chunks when longer
+            const int nc = F.Kt <= 8 ? 1 : (F.Kt + 7) / 8;
+            double acc[T] = {0.0};
+            for (int ch = 0; ch < nc; ch++) {
+                double p[T] = {0.0};
+                for (int K = ch * 8; K < (nc == 1 ? F.Kt : std::min(F.Kt, ch * 8 + 8)); K++) {
+                    const double *L = tile(S, F, I, K);
+                    for (int c = 0; c < T; c++)
+                        for (int r = 0; r < T; r++) p[r] += L[c * T + r] * y[K * T + c];
+                }
+                for (int r = 0; r < T; r++) acc[r] += p[r];
             }
+            for (int r = 0; r < T; r++) v[I * T + r] -= acc[r];
+        }
     }
     for (size_t f = P.fronts.size(); f-- > 0;) {
         const MfFront &F = P.fronts[f];
@@ -127,16 +135,21 @@ int solve_inverted(const MfPlan &P, std::vector<double> &S, const double *b, dou
                 for (int r = 0; r < T; r++) t[K * T + r] -= p[r];
             }
         }
-        for (int K = 0; K < F.Kt; K++) {          // x_K = D_K^{-1} t_K - sum_J Z_KJ t_J
-            const double *Di = tile(S, F, K, K);
-            for (int r = 0; r < T; r++) {
-                double s = 0.0;
-                for (int c = 0; c < T; c++) s += Di[c * T + r] * t[K * T + c];
-                for (int J = K + 1; J < F.Kt; J++) {
-                    const double *Z = tile(S, F, K, J);
-                    for (int c = 0; c < T; c++) s -= Z[c * T + r] * t[J * T + c];
+        for (int K = 0; K < F.Kt; K++) {          // x_K = D_K^{-1} t_K - sum_J Z_KJ t_J,
+            const int m = F.Kt - K;                // 8-tile chunks when longer
+            const int nc = m <= 8 ? 1 : (m + 7) / 8;
+            for (int r = 0; r < T; r++) v[K * T + r] = 0.0;
+            for (int ch = 0; ch < nc; ch++) {
+                const int j1 = nc == 1 ? F.Kt : std::min(F.Kt, K + ch * 8 + 8);
+                for (int r = 0; r < T; r++) {
+                    double s = 0.0;
+                    for (int J = K + ch * 8; J < j1; J++) {
+                        const double *Z = tile(S, F, K, J);
+                        const double sg = J == K ? 1.0 : -1.0;
+                        for (int c = 0; c < T; c++) s += sg * Z[c * T + r] * t[J * T + c];
+                    }
+                    v[K * T + r] += s;
                 }
-                v[K * T + r] = s;
             }
         }
         for (int a = 0; a < F.k; a++) w[var[a]] = v[a];
@@ -166,7 +179,8 @@ int mf_check_stats(int d, int ny, int nx, int leaf, long long *out) {
 // With `inverted`, every front's pivot block is inverted after its
 // factorisation and the sweeps take the device's inverted form: y_P = v_P -
 // Y v_P, ring products in partial sums of 16 tiles, x_K = D_K^{-1} t_K -
-// sum_{J>K} Z_KJ t_J.
+// sum_{J>K} Z_KJ t_J; update rows and pivot rows of more than 8 tiles sum
+// 8-tile chunk partials in chunk order.
 int mf_check_solve(int d, int ny, int nx, int leaf, const int *cols, const double *vals,
                    long long rows, int ell, const double *b, double *x, int inverted) {
     MfPlan P;
