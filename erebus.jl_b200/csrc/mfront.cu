@@ -1074,6 +1074,15 @@ struct MfBwdCursor {
     }
 };
 
+// The next front's gather (this CTA's front fi + G, when its record is in
+// the batch) is prefetched into registers while the current front's tiles
+// stream: its index loads right after the current front's gather, its value
+// loads after the first tile, and the sums, in the gather's order, when it
+// starts.  Thread t holds elements t + j LU_THREADS, j < MF_PF: fronts of
+// up to MF_PF LU_THREADS entries (the levels with several fronts per CTA have
+// at most 640) are prefetched, larger ones gathered when they start.
+constexpr int MF_PF = 3;
+
 template <class T>
 __device__ void mf_fwd_level_s(const MfView &V, int fb, int fe, const double *w, MfSolveSmem &S,
                                uint32_t *uses, int *err) {
@@ -1097,6 +1106,9 @@ __device__ void mf_fwd_level_s(const MfView &V, int fb, int fe, const double *w,
             mf_fetch(S, q, p);
         }
     }
+    int pg[MF_PF], pm0[MF_PF], pm1[MF_PF];   // next front: indices
+    double pw[MF_PF], pc0[MF_PF], pc1[MF_PF];  // next front: values
+    bool have = false;   // the current front's gather is in the registers
     int sl = 0, q = 0;
     for (int fi = fi0; fi < fe; fi += G, q++) {
         if (q == MF_LF_MAX) {   // every thread is past the batch's last front
@@ -1105,7 +1117,18 @@ __device__ void mf_fwd_level_s(const MfView &V, int fb, int fe, const double *w,
             if (threadIdx.x == 0) cur.lf0 = fi;
         }
         const MfLf &f = S.lf[q];
-        {
+        if (have) {
+#pragma unroll
+            for (int j = 0; j < MF_PF; j++) {
+                const int a = threadIdx.x + j * LU_THREADS;
+                if (a < f.M) {
+                    double s = pw[j];
+                    if (pm0[j] >= 0) s += pc0[j];
+                    if (pm1[j] >= 0) s += pc1[j];
+                    vs[a] = s;
+                }
+            }
+        } else {
             const int *var = V.vars + f.var_off, *map = V.eamap + f.map_off;
             const long long c0v = f.c0v, c1v = f.c1v;
             for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
@@ -1123,6 +1146,32 @@ __device__ void mf_fwd_level_s(const MfView &V, int fb, int fe, const double *w,
             }
         }
         __syncthreads();
+        // the next front's indices
+        const bool next =
+            q + 1 < MF_LF_MAX && fi + G < fe && S.lf[q + 1].M <= MF_PF * LU_THREADS;
+        if (next) {
+            const MfLf &nf = S.lf[q + 1];
+            const int *var = V.vars + nf.var_off, *map = V.eamap + nf.map_off;
+#pragma unroll
+            for (int j = 0; j < MF_PF; j++) {
+                const int a = threadIdx.x + j * LU_THREADS;
+                pg[j] = pm0[j] = pm1[j] = -1;
+                if (a < nf.M) {
+                    pg[j] = a < nf.Kp ? var[a] : -1;
+                    if (nf.c0v >= 0) pm0[j] = map[2 * a];
+                    if (nf.c1v >= 0) pm1[j] = map[2 * a + 1];
+                }
+            }
+        }
+        auto values = [&]() {   // the next front's value loads
+            const MfLf &nf = S.lf[q + 1];
+#pragma unroll
+            for (int j = 0; j < MF_PF; j++) {
+                pw[j] = pg[j] >= 0 ? __ldcg(&w[pg[j]]) : 0.0;
+                pc0[j] = pm0[j] >= 0 ? __ldcg(&V.vec[nf.c0v + pm0[j]]) : 0.0;
+                pc1[j] = pm1[j] >= 0 ? __ldcg(&V.vec[nf.c1v + pm1[j]]) : 0.0;
+            }
+        };
         int n = 0;
         for (int K = 0; K < f.Kt; K++) n += f.Mt - K - 1;
         int K = 0, I = 1, b = 0;
@@ -1143,7 +1192,10 @@ __device__ void mf_fwd_level_s(const MfView &V, int fb, int fe, const double *w,
             }
             sl = sl + 1 == NS ? 0 : sl + 1;
             I++;
+            if (next && t == 0) values();
         }
+        if (next && n == 0) values();
+        have = next;
         __syncthreads();
         double *v = V.vec + f.vec_off;
         for (int a = threadIdx.x; a < f.M; a += blockDim.x) __stcg(&v[a], vs[a]);
@@ -1182,6 +1234,10 @@ __device__ void mf_bwd_level_s(const MfView &V, int fb, int fe, double *w, MfSol
         }
         sl = sl + 1 == NS ? 0 : sl + 1;
     };
+    // the next front's vector, prefetched as in mf_fwd_level_s
+    int pg[MF_PF];
+    double pv[MF_PF];
+    bool have = false;
     int q = 0;
     for (int fi = fi0; fi < fe; fi += G, q++) {
         if (q == MF_LF_MAX) {   // every thread is past the batch's last front
@@ -1192,15 +1248,47 @@ __device__ void mf_bwd_level_s(const MfView &V, int fb, int fe, double *w, MfSol
         const MfLf &f = S.lf[q];
         double *v = V.vec + f.vec_off;
         const int *var = V.vars + f.var_off;
-        for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
-            if (a < f.Kp) {
-                vs[a] = __ldcg(&v[a]);
-            } else {
-                int g = var[a];
-                vs[a] = g >= 0 ? __ldcg(&w[g]) : 0.0;
+        if (have) {
+#pragma unroll
+            for (int j = 0; j < MF_PF; j++) {
+                const int a = threadIdx.x + j * LU_THREADS;
+                if (a < f.M) vs[a] = pv[j];
+            }
+        } else {
+            for (int a = threadIdx.x; a < f.M; a += blockDim.x) {
+                if (a < f.Kp) {
+                    vs[a] = __ldcg(&v[a]);
+                } else {
+                    int g = var[a];
+                    vs[a] = g >= 0 ? __ldcg(&w[g]) : 0.0;
+                }
             }
         }
         __syncthreads();
+        // the next front's ring indices (-2: a pivot-part entry, -1: none)
+        const bool next =
+            q + 1 < MF_LF_MAX && fi + G < fe && S.lf[q + 1].M <= MF_PF * LU_THREADS;
+        if (next) {
+            const MfLf &nf = S.lf[q + 1];
+            const int *nvar = V.vars + nf.var_off;
+#pragma unroll
+            for (int j = 0; j < MF_PF; j++) {
+                const int a = threadIdx.x + j * LU_THREADS;
+                pg[j] = a >= nf.M ? -1 : a < nf.Kp ? -2 : nvar[a];
+            }
+        }
+        bool fetched = !next;
+        auto values = [&]() {   // the next front's value loads
+            if (fetched) return;
+            fetched = true;
+            const MfLf &nf = S.lf[q + 1];
+            const double *nv = V.vec + nf.vec_off;
+#pragma unroll
+            for (int j = 0; j < MF_PF; j++) {
+                const int a = threadIdx.x + j * LU_THREADS;
+                pv[j] = pg[j] == -2 ? __ldcg(&nv[a]) : pg[j] >= 0 ? __ldcg(&w[pg[j]]) : 0.0;
+            }
+        };
         const int nr = f.Mt - f.Kt;
         if (nr > 0) {   // rows K < Kt minus the ring products
             for (int K = 0; K < f.Kt; K++) {
@@ -1211,6 +1299,7 @@ __device__ void mf_bwd_level_s(const MfView &V, int fb, int fe, double *w, MfSol
                     acc += mf_quarter(mf_slot<T>(S, sl), vs + (f.Kt + j) * 64);
                     __syncthreads();
                     refill();
+                    values();
                 }
                 const double t = mf_reduce_rows(S, acc);
                 if (threadIdx.x < 64) vs[K * 64 + threadIdx.x] -= t;
@@ -1240,8 +1329,11 @@ __device__ void mf_bwd_level_s(const MfView &V, int fb, int fe, double *w, MfSol
                     refill();
                 }
                 b ^= 1;
+                values();
             }
         }
+        values();
+        have = next;
         __syncthreads();
     }
 }
