@@ -514,8 +514,9 @@ constexpr int MF_SLOTS = 3;
 
 // A front of a one-front-per-CTA level whose vector has at most MF_VS_MAX
 // entries keeps it in shared memory for the whole sweep, so a tile costs
-// one CTA barrier and no round trip to L2.
-constexpr int MF_VS_MAX = 1024;
+// one CTA barrier and no round trip to L2 (20 row blocks: level 6 of the
+// 401 x 401 Stokes-Darcy tree has fronts of 18).
+constexpr int MF_VS_MAX = 1280;
 
 // What the one-front-per-CTA sweeps read of a front's descriptor.  A CTA
 // loads the records of up to MF_LF_MAX of its fronts of a level at once (one
@@ -533,7 +534,6 @@ struct MfSolveSmem {
     unsigned long long bar[MF_SLOTS];
     double part[2][4][64];  // quarter partial sums (two buffers, alternating tiles)
     double x[64];          // vector piece the current tile multiplies
-    double y[64];
     double vs[MF_VS_MAX];  // the front vector of a front swept by one CTA
     union {
         int2 km[MF_KM_MAX];   // cooperative levels: (Kt, Mt) of the level's fronts
@@ -547,6 +547,11 @@ static_assert(sizeof(MfSolveSmem) <= 113 * 1024, "solve shared memory");
 __device__ __forceinline__ uint32_t mf_smem(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
+
+// Vector piece of the sweeps that keep the front vector in global memory:
+// the second partial-sum buffer, which only the shared-memory sweeps'
+// one-barrier reductions (mf_reduce_rows1) use.
+__device__ __forceinline__ double *mf_y(MfSolveSmem &S) { return S.part[1][0]; }
 
 // Tile slots in flight per CTA (three for either element type: six FP32
 // slots in the same storage measured no faster) and slot sl's tile.
@@ -717,10 +722,10 @@ __device__ void mf_fwd_front(const MfView &V, const MfFront &f, double *v, int i
                 I = K + 1;
             }
             if (I == K + 1) {   // first tile of column K: y_K
-                if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
+                if (threadIdx.x < 64) mf_y(S)[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
                 __syncthreads();
             }
-            double t = mf_reduce_rows(S, mf_quarter(Tt, S.y));
+            double t = mf_reduce_rows(S, mf_quarter(Tt, mf_y(S)));
             if (threadIdx.x < 64) {
                 double *d = &v[I * 64 + threadIdx.x];
                 __stcg(d, __ldcg(d) - t);
@@ -780,9 +785,9 @@ __device__ void mf_bwd_front(const MfView &V, const MfFront &f, double *v, doubl
                 j = 0;
             }
             if (j == 0) {   // x_K = D_K^{-1} v_K
-                if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
+                if (threadIdx.x < 64) mf_y(S)[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]);
                 __syncthreads();
-                double x = mf_reduce_rows(S, mf_quarter(Tt, S.y));
+                double x = mf_reduce_rows(S, mf_quarter(Tt, mf_y(S)));
                 if (threadIdx.x < 64) {
                     const int r = threadIdx.x, a = K * 64 + r;
                     S.x[r] = x;
@@ -1455,9 +1460,9 @@ __device__ void mf_bwd_row(const MfView &V, const MfFront &f, double *w, int K, 
                 acc += mf_quarter(Tt, S.x);
             } else {   // the diagonal tile holds D_K^{-1}
                 double t = mf_reduce_rows(S, acc);
-                if (threadIdx.x < 64) S.y[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]) - t;
+                if (threadIdx.x < 64) mf_y(S)[threadIdx.x] = __ldcg(&v[K * 64 + threadIdx.x]) - t;
                 __syncthreads();
-                double x = mf_reduce_rows(S, mf_quarter(Tt, S.y));
+                double x = mf_reduce_rows(S, mf_quarter(Tt, mf_y(S)));
                 if (threadIdx.x < 64) {
                     const int a = K * 64 + threadIdx.x;
                     __stcg(&v[a], x);
@@ -1478,9 +1483,10 @@ __device__ void mf_bwd_row(const MfView &V, const MfFront &f, double *w, int K, 
 // v is gathered where it is read (children's update parts and the right-
 // hand side), so each sweep of a level takes two phases, and every task is
 // one row block or a chunk of one: no task waits for another inside a phase.
-constexpr int MF_XG = MF_VS_MAX / 64;    // vector pieces staged in shared memory at a time
+constexpr int MF_XG = 16;                // vector pieces staged in shared memory at a time
 constexpr int MF_RING_CHUNK = MF_XG;      // ring tiles per backward partial sum
 static_assert(MF_XG * 64 == 4 * LU_THREADS, "staging: four elements per thread");
+static_assert(MF_XG * 64 <= MF_VS_MAX, "staging area");
 
 __host__ __device__ __forceinline__ int mf_ring_chunks(int nr) {
     return (nr + MF_RING_CHUNK - 1) / MF_RING_CHUNK;
