@@ -18,21 +18,34 @@ static __device__ __forceinline__ unsigned long long globaltimer() {
 
 // Sense-reversing grid barrier over all CTAs of a cooperative launch.
 // bar[0] = arrival count, bar[1] = generation.  A wait that exceeds the
-// timeout sets *err and returns.
+// timeout sets *err and returns.  Thread 0 of each CTA arrives with an
+// acquire-release add after the CTA barrier (the release carries the whole
+// CTA's earlier writes), the last arrival bumps the generation with a
+// release, and the others spin on it with acquire loads: 2.05 us per barrier
+// over 296 CTAs on a B200, against 2.45-2.7 us with full fences around
+// relaxed atomics (a two-level arrival tree measured 2.8 us: the cost is
+// round trips, not contention on the counter).
 static __device__ void grid_barrier(unsigned int *bar, int *err) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned int *vgen = bar + 1;
-        unsigned int gen = *vgen;
-        __threadfence();
-        unsigned int arrived = atomicAdd(bar, 1u);
+        unsigned int gen, arrived;
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(gen) : "l"(bar + 1) : "memory");
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                     : "=r"(arrived)
+                     : "l"(bar)
+                     : "memory");
         if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
+            asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(bar), "r"(0u) : "memory");
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
         } else {
-            unsigned long long t0 = globaltimer();
-            while (*vgen == gen) {
+            const unsigned long long t0 = globaltimer();
+            for (;;) {
+                unsigned int g;
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];"
+                             : "=r"(g)
+                             : "l"(bar + 1)
+                             : "memory");
+                if (g != gen) break;
                 if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
                     atomicExch(err, 1);
                     break;
@@ -40,7 +53,6 @@ static __device__ void grid_barrier(unsigned int *bar, int *err) {
                 __nanosleep(64);
             }
         }
-        __threadfence();
     }
     __syncthreads();
 }
