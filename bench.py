@@ -426,9 +426,9 @@ NCU_TRAFFIC = {
 }
 # The triangular solve reads every factor tile once, so its traffic grows with
 # the factor bytes: captured at 141x141 (k_mf_solve<double>: 0.80 GB against
-# 0.79 GB of factors; k_mf_solve<float>: 0.409 GB against 0.393 GB), the
+# 0.79 GB of factors; k_mf_solve<float>: 0.4085 GB against 0.3932 GB), the
 # ratio scales the factor bytes of any workload to a per-launch figure.
-NCU_SOLVE_TRAFFIC_RATIO = {"fp64": 0.80 / 0.79, "fp32": 0.4094 / 0.3932}
+NCU_SOLVE_TRAFFIC_RATIO = {"fp64": 0.80 / 0.79, "fp32": 0.4085 / 0.3932}
 
 
 def roofline(args, res, hbm, hbm_src, f64):
