@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "mf_plan.h"
+#include "mf_tasks.h"
 #include "solver.cuh"
 #include "tiles.cuh"
 
@@ -1484,40 +1485,11 @@ __device__ void mf_bwd_row(const MfView &V, const MfFront &f, double *w, int K, 
 // hand side), so each sweep of a level takes two phases, and every task is
 // one row block or a chunk of one: no task waits for another inside a phase.
 constexpr int MF_XG = 16;                // vector pieces staged in shared memory at a time
-constexpr int MF_RING_CHUNK = MF_XG;      // ring tiles per backward partial sum
 static_assert(MF_XG * 64 == 4 * LU_THREADS, "staging: four elements per thread");
 static_assert(MF_XG * 64 <= MF_VS_MAX, "staging area");
+static_assert(MF_RING_CHUNK == MF_XG, "a B1 task stages its ring pieces once");
 
-__host__ __device__ __forceinline__ int mf_ring_chunks(int nr) {
-    return (nr + MF_RING_CHUNK - 1) / MF_RING_CHUNK;
-}
-
-// F1 splits pivot row block I's products over K < I into chunks of
-// MF_F1_CHUNK tiles (the root's last row would stream 37 tiles through one
-// CTA): chunk 0 stores y_I's gathered entries minus its products in vec2,
-// chunks 1.. store their products as partial sums, and readers of y
-// subtract those in chunk order.
-constexpr int MF_F1_CHUNK = 8;
-__host__ __device__ __forceinline__ int mf_f1_chunks(int I) {
-    return I <= MF_F1_CHUNK ? 1 : (I + MF_F1_CHUNK - 1) / MF_F1_CHUNK;
-}
-// F1 tasks of a front: sum over I < Kt of mf_f1_chunks(I), i.e. 1 (I = 0)
-// plus sum_{I=1}^{n} ceil(I / 8), n = Kt - 1
-__host__ __device__ __forceinline__ int mf_f1_tasks(int Kt) {
-    if (Kt <= 0) return 0;
-    const int n = Kt - 1, q = n / MF_F1_CHUNK, r = n % MF_F1_CHUNK;
-    return 1 + MF_F1_CHUNK * q * (q + 1) / 2 + r * (q + 1);
-}
-// partial-sum slots per pivot row block (the chunks after the first)
-__host__ __device__ __forceinline__ int mf_f1_slots(int Kt) {
-    return Kt >= 2 ? mf_f1_chunks(Kt - 1) - 1 : 0;
-}
-// offset of pivot row block I's F1 partial ch (>= 1) in V.part: after the
-// front's ring partials
-__device__ __forceinline__ long long mf_f1_part(const MfFront &f, int I, int ch) {
-    return f.poff + (long long)f.Kt * mf_ring_chunks(f.Mt - f.Kt) * 64 +
-           ((long long)I * mf_f1_slots(f.Kt) + ch - 1) * 64;
-}
+// The task maps, chunk sizes and partial-sum offsets are in mf_tasks.h.
 // element c of y_K
 __device__ __forceinline__ double mf_inv_y(const MfView &V, const MfFront &f, int K, int c) {
     double y = __ldcg(&V.vec2[f.vec_off + K * 64 + c]);
@@ -1527,33 +1499,13 @@ __device__ __forceinline__ double mf_inv_y(const MfView &V, const MfFront &f, in
 }
 
 // Update rows (F2, Kt tiles each) and pivot rows (B2, Kt - K tiles) of more
-// than MF_F1_CHUNK tiles are split into chunks of MF_F1_CHUNK tiles, each a
-// task of its own (the root's first pivot row would stream 38 tiles through
-// one CTA).  Every chunk stores its partial row product; the chunk that
-// arrives last (a count per row block, in V.flags, which the inverted form
-// does not otherwise use) adds the partials in chunk order and writes the
-// row, so the result does not depend on which CTA finishes last.
-__host__ __device__ __forceinline__ int mf_row_chunks(int n) {
-    return n <= MF_F1_CHUNK ? 1 : (n + MF_F1_CHUNK - 1) / MF_F1_CHUNK;
-}
-// B2 tasks of a front: sum over K < Kt of mf_row_chunks(Kt - K), i.e.
-// sum_{m=1}^{Kt} ceil(m / 8)
-__host__ __device__ __forceinline__ int mf_b2_tasks(int Kt) {
-    if (Kt <= 0) return 0;
-    const int q = Kt / MF_F1_CHUNK, r = Kt % MF_F1_CHUNK;
-    return MF_F1_CHUNK * q * (q + 1) / 2 + r * (q + 1);
-}
-// partial-sum slots of a front's chunked rows: chunks of every row block
-__host__ __device__ __forceinline__ long long mf_row_slots(int Kt, int Mt) {
-    return Kt > MF_F1_CHUNK ? (long long)Mt * mf_row_chunks(Kt) : 0;
-}
-// offset of chunk ch of row block I's partial in V.part: after the ring and
-// F1 partials
-__device__ __forceinline__ long long mf_row_part(const MfFront &f, int I, int ch) {
-    return f.poff +
-           (long long)f.Kt * (mf_ring_chunks(f.Mt - f.Kt) + mf_f1_slots(f.Kt)) * 64 +
-           ((long long)I * mf_row_chunks(f.Kt) + ch) * 64;
-}
+// than MF_F1_CHUNK tiles are split into chunks of MF_F1_CHUNK tiles on the
+// levels that chunk long rows, each chunk a task of its own (the root's first
+// pivot row would stream 38 tiles through one CTA).  Every chunk stores its
+// partial row product; the chunk that arrives last (a count per row block, in
+// V.flags, which the inverted form does not otherwise use) adds the partials
+// in chunk order and writes the row, so the result does not depend on which
+// CTA finishes last.
 // Called by all threads after threads 0..63 stored their chunk's partial:
 // counts the chunk in *cnt and returns, in every thread, whether it was the
 // last of the row's nch.  The last one resets the count for the next solve
@@ -1614,9 +1566,8 @@ __device__ double mf_row_tiles(MfSolveSmem &S, uint32_t *uses, int n, Tile tile,
 template <class T>
 __device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, int u,
                           MfSolveSmem &S, uint32_t *uses, int *err) {
-    int I = 0;
-    while (u >= mf_f1_chunks(I)) u -= mf_f1_chunks(I++);
-    const int ch = u, k0 = ch * MF_F1_CHUNK, n = min(I, k0 + MF_F1_CHUNK) - k0;
+    int I, ch, k0, n;
+    mf_f1_task(f.Kt, u, I, ch, k0, n);
     const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
     MfFront C0, C1;
     if (h0) C0 = V.fr[f.c0];
@@ -1640,15 +1591,15 @@ __device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, in
     }
 }
 
-// F2: chunk ch of nrc of update row block I (>= Kt) of front f, tiles K in
-// [8 ch, 8 ch + 8) (all Kt when nrc = 1): v_I = gathered entries
-// minus sum_K L_IK y_K.  Chunk 0's partial holds the gathered entries minus
-// its products, the later ones their products.
+// F2 task u of front f with nrc chunks per row: chunk ch of update row block
+// I (>= Kt), tiles K in [8 ch, 8 ch + 8) (all Kt when nrc = 1): v_I =
+// gathered entries minus sum_K L_IK y_K.  Chunk 0's partial holds the
+// gathered entries minus its products, the later ones their products.
 template <class T>
-__device__ void mf_inv_f2(const MfView &V, const MfFront &f, const double *w, int I, int ch,
-                          int nrc, MfSolveSmem &S, uint32_t *uses, int *err) {
-    const int k0 = ch * MF_F1_CHUNK;
-    const int n = nrc == 1 ? f.Kt : min(MF_F1_CHUNK, f.Kt - k0);
+__device__ void mf_inv_f2(const MfView &V, const MfFront &f, const double *w, int u, int nrc,
+                          MfSolveSmem &S, uint32_t *uses, int *err) {
+    int I, ch, k0, n;
+    mf_f2_task(f.Kt, nrc, u, I, ch, k0, n);
     const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
     MfFront C0, C1;
     if (h0) C0 = V.fr[f.c0];
@@ -1678,12 +1629,12 @@ __device__ void mf_inv_f2(const MfView &V, const MfFront &f, const double *w, in
     }
 }
 
-// B1: ring tiles [Kt + 16 ch, ...) of pivot row block K of front f.
+// B1 task u of front f: ring tiles [Kt + 16 ch, ...) of pivot row block K.
 template <class T>
-__device__ void mf_inv_b1(const MfView &V, const MfFront &f, const double *w, int K, int ch,
+__device__ void mf_inv_b1(const MfView &V, const MfFront &f, const double *w, int u,
                           MfSolveSmem &S, uint32_t *uses, int *err) {
-    const int nr = f.Mt - f.Kt, nch = mf_ring_chunks(nr), j0 = f.Kt + ch * MF_RING_CHUNK;
-    const int n = min(MF_RING_CHUNK, f.Mt - j0);
+    int K, ch, j0, n;
+    mf_b1_task(f.Kt, f.Mt, u, K, ch, j0, n);
     const int *var = V.vars + f.var_off;
     const double acc = mf_row_tiles<T>(
         S, uses, n, [&](int j) { return (const T *)ftile<T>(V, f, K, j0 + j); },
@@ -1693,28 +1644,27 @@ __device__ void mf_inv_b1(const MfView &V, const MfFront &f, const double *w, in
         },
         [](int) { return 1.0; }, []() {}, err);
     const double t = mf_reduce_rows(S, acc);
-    if (threadIdx.x < 64)
-        __stcg(&V.part[f.poff + ((long long)K * nch + ch) * 64 + threadIdx.x], t);
+    if (threadIdx.x < 64) __stcg(&V.part[mf_ring_part(f, K, ch) + threadIdx.x], t);
 }
 
-// B2: chunk ch of pivot row block K of front f, tiles (K, K + i) for i in
+// B2 task u of front f: chunk ch of pivot row block K, tiles (K, K + i) for i in
 // [8 ch, 8 ch + 8) (all Kt - K when the row has one chunk or the level is not
 // `chunked`); the solution
 // x_K = D_K^{-1} t_K - sum_{J>K} Z_KJ t_J goes to w.
 template <class T>
-__device__ void mf_inv_b2(const MfView &V, const MfFront &f, double *w, int K, int ch,
-                          bool chunked, MfSolveSmem &S, uint32_t *uses, int *err) {
+__device__ void mf_inv_b2(const MfView &V, const MfFront &f, double *w, int u, bool chunked,
+                          MfSolveSmem &S, uint32_t *uses, int *err) {
     const int nch = mf_ring_chunks(f.Mt - f.Kt);
     const int *var = V.vars + f.var_off;
-    const int m = f.Kt - K, nrc = chunked ? mf_row_chunks(m) : 1, i0 = ch * MF_F1_CHUNK;
-    const int n = nrc == 1 ? m : min(MF_F1_CHUNK, m - i0);
+    int K, ch, nrc, i0, n;
+    mf_b2_task(f.Kt, chunked, u, K, ch, nrc, i0, n);
     const double acc = mf_row_tiles<T>(
         S, uses, n, [&](int i) { return (const T *)ftile<T>(V, f, K, K + i0 + i); },
         [&](int i, int c) {
             const int J = K + i0 + i;
             double t = mf_inv_y(V, f, J, c);
             if (nch > 0) {
-                const double *pp = V.part + f.poff + (long long)J * nch * 64 + c;
+                const double *pp = V.part + mf_ring_part(f, J, 0) + c;
                 for (int q = 0; q < nch; q++) t -= __ldcg(&pp[q * 64]);
             }
             return t;
@@ -1778,10 +1728,9 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
             const bool cf = V.lvl_mode[p] & MF_CHUNK_F2;
             mf_for_tasks(
                 V, fb, fe, S.km,
-                [cf](int Kt, int Mt) { return (Mt - Kt) * (cf ? mf_row_chunks(Kt) : 1); },
+                [cf](int Kt, int Mt) { return mf_f2_tasks(Kt, Mt, cf ? mf_row_chunks(Kt) : 1); },
                 [&](const MfFront &f, int u) {
-                    const int nrc = cf ? mf_row_chunks(f.Kt) : 1;
-                    mf_inv_f2<T>(V, f, w, f.Kt + u / nrc, u % nrc, nrc, S, uses, err);
+                    mf_inv_f2<T>(V, f, w, u, cf ? mf_row_chunks(f.Kt) : 1, S, uses, err);
                 });
         } else {
             // one task per row block, in increasing order within each front
@@ -1819,25 +1768,13 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
             }
         } else if (V.inv) {
             mf_for_tasks(
-                V, fb, fe, S.km, [](int Kt, int Mt) { return Kt * mf_ring_chunks(Mt - Kt); },
-                [&](const MfFront &f, int u) {
-                    const int nch = mf_ring_chunks(f.Mt - f.Kt);
-                    mf_inv_b1<T>(V, f, w, u / nch, u % nch, S, uses, err);
-                });
+                V, fb, fe, S.km, [](int Kt, int Mt) { return mf_b1_tasks(Kt, Mt); },
+                [&](const MfFront &f, int u) { mf_inv_b1<T>(V, f, w, u, S, uses, err); });
             grid_barrier(bar, err);
             const bool cb = V.lvl_mode[p] & MF_CHUNK_B2;
             mf_for_tasks(
-                V, fb, fe, S.km, [cb](int Kt, int) { return cb ? mf_b2_tasks(Kt) : Kt; },
-                [&](const MfFront &f, int u) {
-                    int K = 0;
-                    if (cb) {
-                        while (u >= mf_row_chunks(f.Kt - K)) u -= mf_row_chunks(f.Kt - K++);
-                    } else {
-                        K = u;
-                        u = 0;
-                    }
-                    mf_inv_b2<T>(V, f, w, K, u, cb, S, uses, err);
-                });
+                V, fb, fe, S.km, [cb](int Kt, int) { return mf_b2_count(Kt, cb); },
+                [&](const MfFront &f, int u) { mf_inv_b2<T>(V, f, w, u, cb, S, uses, err); });
         } else {
             // one task per pivot row block, the last first
             mf_for_tasks(
@@ -2027,9 +1964,7 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
         if (modes[p] & MF_SOLVE_LOCAL) continue;
         for (int fi = P.level_begin[p]; fi < P.level_begin[p + 1]; fi++) {
             MfFront &F = P.fronts[fi];
-            const long long slots = (long long)F.Kt * (mf_ring_chunks(F.Mt - F.Kt) +
-                                                       mf_f1_slots(F.Kt)) +
-                                    mf_row_slots(F.Kt, F.Mt);
+            const long long slots = mf_part_slots(F.Kt, F.Mt);
             if (slots > 0 && F.Kt > 0) {   // ring partials, F1 partials, chunked rows
                 F.poff = poff;
                 poff += slots * 64;

@@ -8,9 +8,12 @@
 // lists, extend-add maps, entry targets) is checked without a GPU.
 #include <cmath>
 #include <cstring>
+#include <set>
+#include <utility>
 #include <vector>
 
 #include "../erebus.jl_b200/csrc/mf_plan.h"
+#include "../erebus.jl_b200/csrc/mf_tasks.h"
 
 using namespace erebus;
 
@@ -277,5 +280,88 @@ int mf_check_solve(int d, int ny, int nx, int leaf, const int *cols, const doubl
     }
     std::memcpy(x, w.data(), sizeof(double) * P.n);
     return 0;
+}
+
+// Checks the cooperative solve's task maps (mf_tasks.h, the decoders the
+// device solver runs) for every (Kt, Mt) with Kt <= kt_max and Kt <= Mt <=
+// Kt + mt_extra (Mt >= 1), and for every front of the plans of the 41 x 41,
+// 141 x 141 and 401 x 401 grids: each phase's tasks cover the phase's tiles
+// exactly once, and every partial-sum slot (B1 ring partials, F1 chunks,
+// chunked F2 and B2 rows) is used once and lies inside the front's storage.
+// Returns the number of failures.
+int mf_check_tasks(int kt_max, int mt_extra) {
+    int fails = 0;
+    auto check = [&](int Kt, int Mt) {
+        MfFront f{};
+        f.Kt = Kt;
+        f.Mt = Mt;
+        f.poff = 640;
+        const long long end = f.poff + 64 * mf_part_slots(Kt, Mt);
+        std::set<long long> used;
+        auto slot = [&](long long o) {
+            if (o < f.poff || o + 64 > end || !used.insert(o).second) fails++;
+        };
+        std::set<std::pair<int, int>> cov;
+        auto tile = [&](int I, int J) {
+            if (!cov.insert({I, J}).second) fails++;
+        };
+        // B1: ring tiles of the pivot rows
+        for (int u = 0; u < mf_b1_tasks(Kt, Mt); u++) {
+            int K, ch, j0, n;
+            mf_b1_task(Kt, Mt, u, K, ch, j0, n);
+            if (K < 0 || K >= Kt || n < 1 || j0 < Kt || j0 + n > Mt) fails++;
+            for (int j = 0; j < n; j++) tile(K, j0 + j);
+            slot(mf_ring_part(f, K, ch));
+        }
+        if ((long long)cov.size() != (long long)Kt * (Mt - Kt)) fails++;
+        // F1: tiles (I, K), K < I < Kt
+        cov.clear();
+        for (int u = 0; u < mf_f1_tasks(Kt); u++) {
+            int I, ch, k0, n;
+            mf_f1_task(Kt, u, I, ch, k0, n);
+            if (I < 0 || I >= Kt || ch >= mf_f1_chunks(I) || n < 0 || k0 + n > I) fails++;
+            for (int i = 0; i < n; i++) tile(I, k0 + i);
+            if (ch >= 1) slot(mf_f1_part(f, I, ch));
+        }
+        if ((long long)cov.size() != (long long)Kt * (Kt - 1) / 2) fails++;
+        // F2 and B2, one task per row and chunked
+        for (int chunked = 0; chunked < 2; chunked++) {
+            std::set<long long> used0 = used;
+            const int nrc = chunked ? mf_row_chunks(Kt) : 1;
+            cov.clear();
+            for (int u = 0; u < mf_f2_tasks(Kt, Mt, nrc); u++) {
+                int I, ch, k0, n;
+                mf_f2_task(Kt, nrc, u, I, ch, k0, n);
+                if (I < Kt || I >= Mt || (n < 1 && Kt > 0) || k0 + n > Kt) fails++;
+                for (int i = 0; i < n; i++) tile(I, k0 + i);
+                if (nrc > 1) slot(mf_row_part(f, I, ch));
+            }
+            if ((long long)cov.size() != (long long)(Mt - Kt) * Kt) fails++;
+            cov.clear();
+            for (int u = 0; u < mf_b2_count(Kt, chunked); u++) {
+                int K, ch, r, i0, n;
+                mf_b2_task(Kt, chunked, u, K, ch, r, i0, n);
+                if (K < 0 || K >= Kt || ch >= r || n < 1 || K + i0 + n > Kt) fails++;
+                if (r > 1 && r > mf_row_chunks(Kt)) fails++;
+                for (int i = 0; i < n; i++) tile(K, K + i0 + i);
+                if (r > 1) slot(mf_row_part(f, K, ch));
+            }
+            if ((long long)cov.size() != (long long)Kt * (Kt + 1) / 2) fails++;
+            used = used0;   // the two forms are alternatives
+        }
+    };
+    for (int Kt = 0; Kt <= kt_max; Kt++)
+        for (int Mt = Kt > 1 ? Kt : 1; Mt <= Kt + mt_extra; Mt++) check(Kt, Mt);
+    const int grids[3] = {41, 141, 401};
+    for (int g : grids)
+        for (int d : {6, 1}) {
+            MfPlan P;
+            if (!mf_analyse(P, d, g, g, d == 6 ? 32 : 64)) {
+                fails++;
+                continue;
+            }
+            for (const MfFront &F : P.fronts) check(F.Kt, F.Mt);
+        }
+    return fails;
 }
 }

@@ -31,6 +31,7 @@ def mf(tmp_path_factory):
     L.mf_check_solve.argtypes = [ctypes.c_int] * 4 + [P, P, ctypes.c_longlong, ctypes.c_int,
                                                       P, P, ctypes.c_int]
     L.mf_check_stats.argtypes = [ctypes.c_int] * 4 + [P]
+    L.mf_check_tasks.argtypes = [ctypes.c_int, ctypes.c_int]
     return L
 
 
@@ -144,3 +145,13 @@ def test_stats_of_the_workloads(mf):
         sizes[n1] = out.copy()
     assert sizes[142][2] * 8 < 2.5e9            # bytes of front storage at 141 x 141
     assert sizes[402][2] * 8 < 40e9             # and at 401 x 401
+
+
+def test_cooperative_solve_task_maps(mf):
+    """The task decoders of the cooperative solve levels (mf_tasks.h, compiled
+    into the device solver as they are here): for every front shape up to
+    Kt = 80 row blocks and 90 update row blocks, and every front of the three
+    workloads' plans, each phase (F1, F2, B1, B2; F2 and B2 one task per row
+    and in 8-tile chunks) covers its tiles exactly once, and every partial-sum
+    slot is used once and lies inside the front's storage."""
+    assert mf.mf_check_tasks(80, 90) == 0
