@@ -49,6 +49,7 @@ struct MfView {
     const int *lvl_kt;  // max Kt per level
     const int *lvl_mode;  // per level: MF_FACTOR_LOCAL, MF_SOLVE_LOCAL, ... bits
     int *flags;         // per 64-row block of the front vectors: the solve epoch it is final in
+    int *done;          // per front (at its first row block), F1 and B1 tasks counted done
     double *vec2;       // pivot part of the forward solution (levels with inverted pivot blocks)
     double *part;       // partial sums of the backward ring products (MfFront::poff)
     int inv;            // cooperative solve levels hold inverted pivot blocks
@@ -69,6 +70,7 @@ struct MfDevice {
     int *vars = nullptr, *eamap = nullptr, *lvl = nullptr, *lvl_kt = nullptr;
     int *lvl_mode = nullptr;
     int *flags = nullptr;   // row-block flags of the cooperative solve levels
+    int *done = nullptr;    // per-front counts of the inverted form's F1 and B1 tasks
     int epoch = 0;          // solves launched so far
     // inverted pivot blocks of the cooperative solve levels
     bool inv = false;
@@ -1525,20 +1527,61 @@ __device__ __forceinline__ bool mf_chunk_arrive(int *cnt, int nch, MfSolveSmem &
     return S.last;
 }
 
+// Inside a cooperative level the F2 tasks of a front read only that front's
+// F1 results, and its B2 tasks only its B1 partials, so instead of a grid
+// barrier between the phases each F1 (B1) task counts itself done in the
+// front's count, V.done[2 r] (V.done[2 r + 1]) with r the front's first row
+// block, and an F2 (B2) task waits for its front's count.  The counts grow
+// by the front's task count every solve: solve `epoch` waits for epoch x
+// tasks (compared modulo 2^32).  Every CTA runs all its F1 (B1) tasks before
+// any F2 (B2) task and those wait for nothing, so every wait ends; waits are
+// bounded (2 s; on timeout *err = 3) all the same.
+__device__ __forceinline__ int *mf_done(const MfView &V, const MfFront &f, int phase) {
+    return V.done + 2 * (f.vec_off / 64) + phase;
+}
+// Called by all threads after their outputs are stored.
+__device__ __forceinline__ void mf_count_done(int *cnt) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(cnt, 1);
+}
+// Called by all threads; returns once *cnt has reached `want` (mod 2^32).
+__device__ __forceinline__ void mf_wait_done(const int *cnt, unsigned int want, int *err) {
+    if (threadIdx.x == 0) {
+        unsigned long long t0 = 0;
+        for (int spin = 0;; spin++) {
+            const unsigned int c = (unsigned int)*(volatile const int *)cnt;
+            if ((int)(c - want) >= 0) break;
+            if (*(volatile const int *)err) break;   // the launch is giving up
+            if (spin == 0) {
+                t0 = globaltimer();
+            } else if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
+                atomicExch(err, 3);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
 // Per-thread quarter sums of sum_{i<n} sign(i) T_i x_i: tile(i) points to
 // T_i, piece(i, c) gives element c of x_i; the pieces are staged in
-// S.vs MF_XG at a time while the tiles stream.  first() runs in all threads
-// once, after the first tiles' copies and the first pieces' loads are
-// issued, so the task's own gather overlaps both.
-template <class T, class Tile, class Piece, class Sign, class First>
+// S.vs MF_XG at a time while the tiles stream.  wait() runs in all threads
+// once, after the first tiles' copies are issued and before any piece is
+// read; first() once, after the first pieces' loads are issued, so the
+// task's own gather overlaps them.
+template <class T, class Tile, class Piece, class Sign, class Wait, class First>
 __device__ double mf_row_tiles(MfSolveSmem &S, uint32_t *uses, int n, Tile tile, Piece piece,
-                               Sign sign, First first, int *err) {
+                               Sign sign, Wait wait, First first, int *err) {
     double acc = 0.0;
     if (n == 0) first();
     mf_stream(
         S, uses, n, tile,
         [&](int i, const T *Tt) { acc += sign(i) * mf_quarter(Tt, S.vs + (i % MF_XG) * 64); },
         [&](int i) {
+            if (i == 0) wait();
             if (i % MF_XG == 0) {   // staged while the tiles' copies are in flight; the
                                     // previous tile's barrier has passed
                 const int m = min(n - i, MF_XG) * 64;
@@ -1578,7 +1621,7 @@ __device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, in
         [&](int i, int c) {
             return mf_gather_elem(V, f, w, (k0 + i) * 64 + c, h0, C0, h1, C1);
         },
-        [](int) { return 1.0; },
+        [](int) { return 1.0; }, []() {},
         [&]() {
             if (ch == 0 && threadIdx.x < 64)
                 g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
@@ -1589,6 +1632,7 @@ __device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, in
         if (ch == 0) __stcg(&V.vec2[f.vec_off + I * 64 + threadIdx.x], g - t);
         else __stcg(&V.part[mf_f1_part(f, I, ch) + threadIdx.x], t);
     }
+    mf_count_done(mf_done(V, f, 0));
 }
 
 // F2 task u of front f with nrc chunks per row: chunk ch of update row block
@@ -1597,7 +1641,7 @@ __device__ void mf_inv_f1(const MfView &V, const MfFront &f, const double *w, in
 // gathered entries minus its products, the later ones their products.
 template <class T>
 __device__ void mf_inv_f2(const MfView &V, const MfFront &f, const double *w, int u, int nrc,
-                          MfSolveSmem &S, uint32_t *uses, int *err) {
+                          int epoch, MfSolveSmem &S, uint32_t *uses, int *err) {
     int I, ch, k0, n;
     mf_f2_task(f.Kt, nrc, u, I, ch, k0, n);
     const bool h0 = f.c0 >= 0, h1 = f.c1 >= 0;
@@ -1608,6 +1652,9 @@ __device__ void mf_inv_f2(const MfView &V, const MfFront &f, const double *w, in
     const double acc = mf_row_tiles<T>(
         S, uses, n, [&](int i) { return (const T *)ftile<T>(V, f, I, k0 + i); },
         [&](int i, int c) { return mf_inv_y(V, f, k0 + i, c); }, [](int) { return 1.0; },
+        [&]() {   // the front's pivot rows (F1)
+            mf_wait_done(mf_done(V, f, 0), (unsigned)epoch * (unsigned)mf_f1_tasks(f.Kt), err);
+        },
         [&]() {
             if (ch == 0 && threadIdx.x < 64)
                 g = mf_gather_elem(V, f, w, I * 64 + threadIdx.x, h0, C0, h1, C1);
@@ -1642,9 +1689,10 @@ __device__ void mf_inv_b1(const MfView &V, const MfFront &f, const double *w, in
             const int g = var[(j0 + j) * 64 + c];
             return g >= 0 ? __ldcg(&w[g]) : 0.0;
         },
-        [](int) { return 1.0; }, []() {}, err);
+        [](int) { return 1.0; }, []() {}, []() {}, err);
     const double t = mf_reduce_rows(S, acc);
     if (threadIdx.x < 64) __stcg(&V.part[mf_ring_part(f, K, ch) + threadIdx.x], t);
+    mf_count_done(mf_done(V, f, 1));
 }
 
 // B2 task u of front f: chunk ch of pivot row block K, tiles (K, K + i) for i in
@@ -1653,7 +1701,7 @@ __device__ void mf_inv_b1(const MfView &V, const MfFront &f, const double *w, in
 // x_K = D_K^{-1} t_K - sum_{J>K} Z_KJ t_J goes to w.
 template <class T>
 __device__ void mf_inv_b2(const MfView &V, const MfFront &f, double *w, int u, bool chunked,
-                          MfSolveSmem &S, uint32_t *uses, int *err) {
+                          int epoch, MfSolveSmem &S, uint32_t *uses, int *err) {
     const int nch = mf_ring_chunks(f.Mt - f.Kt);
     const int *var = V.vars + f.var_off;
     int K, ch, nrc, i0, n;
@@ -1669,7 +1717,13 @@ __device__ void mf_inv_b2(const MfView &V, const MfFront &f, double *w, int u, b
             }
             return t;
         },
-        [=](int i) { return i0 + i == 0 ? 1.0 : -1.0; }, []() {}, err);
+        [=](int i) { return i0 + i == 0 ? 1.0 : -1.0; },
+        [&]() {   // the front's ring partials (B1)
+            if (nch > 0)
+                mf_wait_done(mf_done(V, f, 1),
+                             (unsigned)epoch * (unsigned)mf_b1_tasks(f.Kt, f.Mt), err);
+        },
+        []() {}, err);
     double x = mf_reduce_rows(S, acc);
     if (nrc > 1) {
         if (threadIdx.x < 64) __stcg(&V.part[mf_row_part(f, K, ch) + threadIdx.x], x);
@@ -1724,13 +1778,14 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
             mf_for_tasks(
                 V, fb, fe, S.km, [](int Kt, int) { return mf_f1_tasks(Kt); },
                 [&](const MfFront &f, int u) { mf_inv_f1<T>(V, f, w, u, S, uses, err); });
-            grid_barrier(bar, err);
+            // no grid barrier: an F2 task waits for its own front's F1 tasks
             const bool cf = V.lvl_mode[p] & MF_CHUNK_F2;
             mf_for_tasks(
                 V, fb, fe, S.km,
                 [cf](int Kt, int Mt) { return mf_f2_tasks(Kt, Mt, cf ? mf_row_chunks(Kt) : 1); },
                 [&](const MfFront &f, int u) {
-                    mf_inv_f2<T>(V, f, w, u, cf ? mf_row_chunks(f.Kt) : 1, S, uses, err);
+                    mf_inv_f2<T>(V, f, w, u, cf ? mf_row_chunks(f.Kt) : 1, epoch, S, uses,
+                                 err);
                 });
         } else {
             // one task per row block, in increasing order within each front
@@ -1770,11 +1825,13 @@ k_mf_solve(MfView V, double *w, unsigned int *bar, int *err, int epoch) {
             mf_for_tasks(
                 V, fb, fe, S.km, [](int Kt, int Mt) { return mf_b1_tasks(Kt, Mt); },
                 [&](const MfFront &f, int u) { mf_inv_b1<T>(V, f, w, u, S, uses, err); });
-            grid_barrier(bar, err);
+            // no grid barrier: a B2 task waits for its own front's B1 tasks
             const bool cb = V.lvl_mode[p] & MF_CHUNK_B2;
             mf_for_tasks(
                 V, fb, fe, S.km, [cb](int Kt, int) { return mf_b2_count(Kt, cb); },
-                [&](const MfFront &f, int u) { mf_inv_b2<T>(V, f, w, u, cb, S, uses, err); });
+                [&](const MfFront &f, int u) {
+                    mf_inv_b2<T>(V, f, w, u, cb, epoch, S, uses, err);
+                });
         } else {
             // one task per pivot row block, the last first
             mf_for_tasks(
@@ -1801,6 +1858,7 @@ static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
     V.lvl_kt = D.lvl_kt;
     V.lvl_mode = D.lvl_mode;
     V.flags = D.flags;
+    V.done = D.done;
     V.vec2 = D.vec2;
     V.part = D.part;
     V.inv = D.inv ? 1 : 0;
@@ -1814,20 +1872,25 @@ static MfView mf_view(const MfDevice &D, const BandSystem &sys) {
 
 bool mf_is_fp32(const BandSystem &sys) { return sys.mf && sys.mf->fp32; }
 
-// Zeroes the row-block flags (the chunk counts of the inverted form): after
-// a solve that gave up, counts of chunks that never arrived must not carry
-// over into the next solve.
+// Zeroes the row-block flags (the chunk counts of the inverted form) and the
+// per-front task counts, and restarts the epochs: after a solve that gave
+// up, counts of tasks that never finished must not carry over into the next
+// solve.
 void mf_clear_counts(erebus_state *s, BandSystem &sys) {
     MfDevice *D = sys.mf;
     if (!D || !D->flags) return;
     cudaMemsetAsync(D->flags, 0, (D->plan.vec / MF_TILE + 1) * sizeof(int), s->stream);
+    if (D->done)
+        cudaMemsetAsync(D->done, 0, 2 * (D->plan.vec / MF_TILE + 1) * sizeof(int), s->stream);
+    D->epoch = 0;   // the counts restart with the epochs
 }
 
 void mf_release(BandSystem &sys) {
     MfDevice *D = sys.mf;
     if (!D) return;
     void *ps[] = {D->fr, D->F64, D->F32, D->vec, D->vars, D->eamap, D->lvl, D->lvl_kt,
-                  D->lvl_mode, D->flags, D->target, D->expect, D->vec2, D->part, D->inv_list,
+                  D->lvl_mode, D->flags, D->done, D->target, D->expect, D->vec2, D->part,
+                  D->inv_list,
                   D->cvt};
     for (void *p : ps)
         if (p) cudaFree(p);
@@ -1990,6 +2053,10 @@ static int mf_prepare(erebus_state *s, BandSystem &sys, int dofs) {
     if (e == cudaSuccess) e = upload(&D->expect, expect, s->stream);
     if (e == cudaSuccess) e = cudaMalloc(&D->vec, P.vec * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&D->flags, (P.vec / MF_TILE + 1) * sizeof(int));
+    if (e == cudaSuccess && D->inv)
+        e = cudaMalloc(&D->done, 2 * (P.vec / MF_TILE + 1) * sizeof(int));
+    if (e == cudaSuccess && D->inv)
+        e = cudaMemsetAsync(D->done, 0, 2 * (P.vec / MF_TILE + 1) * sizeof(int), s->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(D->flags, 0, (P.vec / MF_TILE + 1) * sizeof(int),
                                               s->stream);
     if (e != cudaSuccess) {
