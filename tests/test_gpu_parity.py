@@ -126,6 +126,10 @@ def test_one_step_parity(pkg, oracle, built_lib, advanced):
     np.testing.assert_array_equal(sg.m["tm"][:n], so.m["tm"][:n])
     for k in ["vx", "vy", "pr", "pf", "qxD", "qyD", "tk2"]:
         assert rel_l2(sg.grid[k], so.grid[k]) <= 1e-8, k
+    # the pressures traced back along the velocities (backtrace_pressures_rk4!,
+    # E:5284-5496) and the P nodes' melt composition (E:1929-1939)
+    for k in ["pr0", "pf0", "ps0", "XWS"]:
+        assert rel_l2(sg.grid[k], so.grid[k]) <= 1e-8, k
     sim.close()
 
 
