@@ -1695,10 +1695,10 @@ __device__ void mf_inv_b1(const MfView &V, const MfFront &f, const double *w, in
     mf_count_done(mf_done(V, f, 1));
 }
 
-// B2 task u of front f: chunk ch of pivot row block K, tiles (K, K + i) for i in
-// [8 ch, 8 ch + 8) (all Kt - K when the row has one chunk or the level is not
-// `chunked`); the solution
-// x_K = D_K^{-1} t_K - sum_{J>K} Z_KJ t_J goes to w.
+// B2 task u of front f: chunk ch of pivot row block K, tiles (K, K + i) for i
+// in [8 ch, 8 ch + 8) (all Kt - K when the row has one chunk or the level is
+// not `chunked`); the solution x_K = D_K^{-1} t_K - sum_{J>K} Z_KJ t_J goes
+// to w.
 template <class T>
 __device__ void mf_inv_b2(const MfView &V, const MfFront &f, double *w, int u, bool chunked,
                           int epoch, MfSolveSmem &S, uint32_t *uses, int *err) {
